@@ -1,0 +1,380 @@
+"""Benchmark of the wind-tunnel LBM hot path on B200.
+
+Workload (default): 512x256x256 = 33.5M cells, FP32 populations, a seeded union of six
+axis-aligned ellipsoids (semi-axes 10-60 cells) resting on a moving ground belt,
+u = 0.05, nu = 0.001 (tau = 0.503), Smagorinsky Cs = 0.16. One bench step is one frame
+of the reference's serving loop: 10 LBM steps, particle advection (2000 streamline
+particles seeded on the inlet plane), packing, a 512x256 speed slice at mid-height,
+surface pressure on every boundary cell and the momentum-exchange force.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line. `value` is aggregate GLUPS over all ranks with the lattice resident
+in HBM; `e2e` is a whole session through the public Solver API (mask and surface upload,
+reset, then K frames each with its outputs read back to pinned host memory). Populations
+(5.1 GB) are far larger than L2, so no flush is needed between steps.
+
+N > 1 runs independent replicas, one tunnel per GPU ("replicas only": independent
+tunnels never exchange data); time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'wind-tunnel_b200'))
+
+STEPS_PER_FRAME = 10
+N_PARTICLES = 2000
+ALGO_BYTES = {'fp32': 152, 'fp16': 76, 'bf16': 76, 'fp64': 304}  # per cell per LBM step
+METRIC = 'GLUPS & % of HBM roofline, FP16-store vs FP32 at stated error; p99 frame ms'
+
+
+def env_int(k, d):
+    return int(os.environ.get(k, d))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+            m = json.load(fh)
+        return float(m['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+def profile_traffic(name):
+    """dram bytes per launch from a committed ncu summary (profiles/<name>), if present."""
+    path = os.path.join(ROOT, 'profiles', name)
+    try:
+        for line in open(path):
+            if line.startswith('traffic_bytes_per_step:'):
+                return float(line.split(':', 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ['clocks.sm', 'clocks.max.sm', 'power.draw', 'clocks_event_reasons.hw_slowdown',
+              'clocks_event_reasons.hw_thermal_slowdown', 'clocks_event_reasons.sw_thermal_slowdown',
+              'clocks_event_reasons.sw_power_cap']
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--id={self.gpu}', '--query-gpu=' + ','.join(self.FIELDS),
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:]):
+                if v.lower().startswith('active'):
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def frame_params(dims):
+    nx, ny, nz = dims
+    return dict(uIn=0.05, tau=3 * 0.001 + 0.5, smag=0.16, steps=STEPS_PER_FRAME,
+                maxAge=2.2 * nx / (0.05 * STEPS_PER_FRAME), lref=40.0,
+                seedX=2.0, seedCy=(ny - 1) / 2, seedCz=(nz - 1) / 2, seedHy=(ny - 4) / 2, seedHz=(nz - 4) / 2,
+                slice=dict(axis=1, index=ny // 2, field=0, vmin=0.0, vmax=1.6), cp=True)
+
+
+def build_workload(scale):
+    import bodies
+    dims, solid, p = bodies.config2(scale=scale)
+    verts, norms = bodies.surface_points(solid, dims)
+    return dims, solid, verts, norms
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import lbm
+
+    dev = torch.device('cuda', local_rank)
+    torch.cuda.set_device(dev)
+    dims, solid, verts, norms = build_workload(args.scale)
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    p = frame_params(dims)
+    prec = args.precision
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident frame loop ----
+    s = lbm.Solver(dims, dev, precision=prec, seed=1234 + rank)
+    s.set_solid(solid)
+    s.set_surface(verts, norms)
+    s.reset(p['uIn'])
+    s.set_particles(N_PARTICLES, p)
+    launches_per_frame = 2 * STEPS_PER_FRAME + 1 + 1 + 1 + 1 + 2  # steps, advect, pack, slice, cp, forces(2)
+
+    def frame_device():
+        s.step(STEPS_PER_FRAME, p)
+        s.launch_frame(p, want_cp=True, copy=False)  # outputs stay on the device
+
+    for _ in range(args.warmup):
+        frame_device()
+    s.synchronize()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize(dev)
+        ev0.record(s.stream)
+        for _ in range(args.steps):
+            frame_device()
+        ev1.record(s.stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    value = world * n * STEPS_PER_FRAME * args.steps / t_dev / 1e9
+
+    # ---- LBM step alone: roofline of the fused step (bulk + face kernels) ----
+    nstep = max(20, args.steps)
+    torch.cuda.synchronize(dev)
+    ev0.record(s.stream)
+    s.step(nstep, p)
+    ev1.record(s.stream)
+    torch.cuda.synchronize(dev)
+    t_step = ev0.elapsed_time(ev1) / 1e3 / nstep
+    hbm, peak_kind = peaks()
+    achieved = ALGO_BYTES[prec] * n / t_step / 1e9
+    traffic = profile_traffic(f'step_{prec}_{nx}x{ny}x{nz}.md')
+    roofline = {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': hbm, 'unit': 'GB/s',
+                'frac': round(achieved / hbm, 4), 'traffic': traffic,
+                'peak_source': f'{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)' if peak_kind == 'measured'
+                else 'fallback 6.65 TB/s', 'kernel': f'wt_step ({prec}) = k_step_bulk + k_step_faces, one LBM step',
+                'algorithmic_bytes_per_cell': ALGO_BYTES[prec], 'step_ms': round(t_step * 1e3, 4),
+                'glups_step_only': round(n / t_step / 1e9, 3)}
+    del s
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the public Solver API, host buffers ----
+    host_solid = torch.from_numpy(solid).pin_memory().numpy()
+    host_verts = torch.from_numpy(verts).pin_memory().numpy()
+    host_norms = torch.from_numpy(norms).pin_memory().numpy()
+    frame_ms = []
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    s = lbm.Solver(dims, dev, precision=prec, seed=99 + rank)
+    s.set_solid(host_solid)
+    s.set_surface(host_verts, host_norms)
+    s.reset(p['uIn'])
+    s.set_particles(N_PARTICLES, p)
+    d2h = 0
+    for _ in range(args.steps):
+        tf = time.perf_counter()
+        s.step(STEPS_PER_FRAME, p)
+        out = s.frame(p, want_cp=True)
+        frame_ms.append((time.perf_counter() - tf) * 1e3)
+        d2h = sum(out[k].nbytes for k in ('parts16', 'parts8', 'slice', 'cp')) + 6 * 8
+    torch.cuda.synchronize(dev)
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    h2d_total = solid.nbytes + verts.nbytes + norms.nbytes + N_PARTICLES * 16
+    e2e = {'value': round(world * n * STEPS_PER_FRAME * args.steps / t_e2e / 1e9, 3), 'unit': 'GLUPS',
+           'h2d_bytes_per_step': int(round(h2d_total / args.steps)), 'd2h_bytes_per_step': int(d2h),
+           'what': 'one session through lbm.Solver: set_solid + set_surface + reset + set_particles, then K frames of '
+                   'step(10) + frame() with outputs copied to pinned host memory',
+           'frame_ms': {'p50': round(float(np.percentile(frame_ms, 50)), 3),
+                        'p99': round(float(np.percentile(frame_ms, 99)), 3)}}
+    del s
+    torch.cuda.empty_cache()
+
+    # ---- storage-precision variants of the step (same workload) ----
+    variants = {}
+    if args.variants and prec == 'fp32':
+        for vp in ('fp16', 'bf16'):
+            v = lbm.Solver(dims, dev, precision=vp)
+            v.set_solid(solid)
+            v.reset(p['uIn'])
+            v.step(5, p)
+            torch.cuda.synchronize(dev)
+            ev0.record(v.stream)
+            v.step(nstep, p)
+            ev1.record(v.stream)
+            torch.cuda.synchronize(dev)
+            tv = ev0.elapsed_time(ev1) / 1e3 / nstep
+            variants[vp] = {'glups_step_only': round(n / tv / 1e9, 3),
+                            'achieved_gbs': round(ALGO_BYTES[vp] * n / tv / 1e9, 1),
+                            'speedup_vs_fp32_step': round(t_step / tv, 3)}
+            del v
+            torch.cuda.empty_cache()
+
+    return dict(value=value, t_dev=t_dev, roofline=roofline, e2e=e2e, clocks=clk.summary(),
+                launches=launches_per_frame * args.steps, dims=dims, n=n, variants=variants)
+
+
+def cpu_baseline(dims, solid, budget_s, threads=None):
+    """The oracle (C++ restatement of the reference kernels, OpenMP) on the host cores:
+    whole-grid LBM steps of the same workload until `budget_s` seconds have been spent."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle
+    cores = oracle.set_threads(threads or os.cpu_count() or 1)
+    L = oracle.Lattice(dims, oracle.F32)
+    L.solid[:] = solid
+    L.reset(0.05)
+    L.step(1, 0.05, 0.503, 0.16)  # warm-up (page faults)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        L.step(1, 0.05, 0.503, 0.16)
+        k += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    n = dims[0] * dims[1] * dims[2]
+    return {'value': round(k * n / dt / 1e9, 5), 'unit': 'GLUPS', 'cores': cores, 'kind': 'port',
+            'sample': f'{k} whole-grid LBM steps of {dims[0]}x{dims[1]}x{dims[2]} (oracle/lbm_oracle.cpp, '
+                      f'OpenMP, {cores} threads); Warp CPU backend unavailable on this box'}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp16', 'bf16', 'fp64'])
+    ap.add_argument('--scale', type=float, default=1.0, help='grid scale (1.0 = 512x256x256)')
+    ap.add_argument('--cpu-budget', type=float, default=12.0)
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-variants', dest='variants', action='store_false')
+    args = ap.parse_args()
+
+    world = env_int('WORLD_SIZE', 1)
+    rank = env_int('RANK', 0)
+    local_rank = env_int('LOCAL_RANK', 0)
+
+    if args.impl == 'reference':
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120),
+                                device_id=torch.device('cuda', local_rank))
+    r = run_ours(args, rank, world, local_rank)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        import bodies
+        dims, solid, _ = bodies.config2(scale=args.scale)
+        cpu = cpu_baseline(dims, solid, args.cpu_budget)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    nx, ny, nz = r['dims']
+    line = {
+        'metric': METRIC, 'value': round(r['value'], 3), 'unit': 'GLUPS', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': round(r['t_dev'] / args.steps * 1e3, 4), 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': {'fp32': 'f32', 'fp16': 'f16-store/f32',
+                                                          'bf16': 'bf16-store/f32', 'fp64': 'f64'}[args.precision],
+        'data': 'synthetic (seeded ellipsoid-union obstacle, PCG64 seed 2024)',
+        'config': {'workload': f'{nx}x{ny}x{nz} D3Q19 regularized-LBM + Smagorinsky, {args.precision} populations, '
+                               f'6-ellipsoid body on moving belt, frame = {STEPS_PER_FRAME} steps + {N_PARTICLES} '
+                               f'particles + {nx}x{nz} slice + surface Cp + forces',
+                   'cells': r['n'], 'steps_per_frame': STEPS_PER_FRAME, 'l2': 'inputs larger than L2 (no flush)',
+                   'parallelism': f'replicas x{world}'},
+        'roofline': r['roofline'], 'cpu_baseline': cpu, 'e2e': r['e2e'], 'clocks': r['clocks'],
+        'gpu_launches': r['launches'], 'precision_variants': r['variants'],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU implementation of the path timed on the host cores: the oracle
+    port (C++ restatement of server/lbm.py's kernels), all threads, one whole-grid LBM step
+    per bench step. Rank 0 only."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import bodies
+    import oracle
+    dims, solid, p = bodies.config2(scale=args.scale)
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    L = oracle.Lattice(dims, oracle.F32)
+    L.solid[:] = solid
+    L.reset(p['uIn'])
+    for _ in range(args.warmup):
+        L.step(1, p['uIn'], p['tau'], p['smag'])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L.step(1, p['uIn'], p['tau'], p['smag'])
+    dt = time.perf_counter() - t0
+    n = dims[0] * dims[1] * dims[2]
+    v = n * args.steps / dt / 1e9
+    nx, ny, nz = dims
+    line = {'impl': 'reference', 'metric': METRIC, 'value': round(v, 5), 'unit': 'GLUPS', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': round(dt / args.steps * 1e3, 3),
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'data': 'synthetic (seeded ellipsoid-union obstacle, PCG64 seed 2024)',
+            'config': {'workload': f'{nx}x{ny}x{nz} D3Q19 regularized-LBM + Smagorinsky, fp32 populations, '
+                                   f'6-ellipsoid body on moving belt', 'cells': n},
+            'cpu_baseline': {'value': round(v, 5), 'unit': 'GLUPS', 'cores': cores, 'kind': 'port',
+                             'sample': f'1 whole-grid LBM step of {nx}x{ny}x{nz} per bench step (oracle port, '
+                                       f'OpenMP {cores} threads); Warp CPU backend unavailable on this box'},
+            'e2e': {'value': round(v, 5), 'unit': 'GLUPS', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,130 @@
+/* wt.h -- C ABI of libwt.so, the B200 (sm_100a) kernels of the wind-tunnel LBM hot path.
+ *
+ * Drop-in boundary: these entry points replace the NVIDIA Warp launches that the
+ * reference Solver (RICKxxROLLING/wind-tunnel, server/lbm.py:398-482) makes. A host
+ * binding (ctypes here; cgo/JNI would bind the same symbols) owns the device buffers
+ * and calls these with raw device pointers, sizes and a cudaStream_t passed as void*.
+ *
+ * Conventions
+ *   - Every function returns 0 (WT_OK) or a negative WT_ERR_* code; wt_last_error()
+ *     gives a message for the calling thread's last failure.
+ *   - Layout is the reference's: cell index idx = x + nx*(y + ny*z), x fastest
+ *     (server/lbm.py:78-80); populations are SoA, population i of cell idx at f[i*n + idx]
+ *     (server/lbm.py:404); mac is 4 reals per cell (ux, uy, uz, rho) (server/lbm.py:406);
+ *     solid is one byte per cell: 0 fluid, 1 static solid, 2 moving belt, any other
+ *     non-zero value a static solid that force sums ignore (server/lbm.py:81, 115-124, 188).
+ *   - Kernels are asynchronous on `stream` (NULL = legacy default stream). Nothing here
+ *     allocates device memory in a hot call; scratch is passed in by the caller.
+ *   - Scalar parameters are passed as double and rounded once to the kernel's arithmetic
+ *     type (float, as Warp rounds the reference's Python floats; double for WT_F64).
+ *   - Storage precision: WT_F32 stores populations as float (the reference's form);
+ *     WT_F16 / WT_BF16 store f_i - w_i as half / bfloat16 (rounded to nearest even) with
+ *     all collision arithmetic in float; WT_F64 stores and computes in double (the
+ *     oracle run). mac is float for WT_F32/F16/BF16 and double for WT_F64.
+ */
+#ifndef WT_H
+#define WT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WT_ABI_VERSION 1
+
+enum {
+    WT_OK = 0,
+    WT_ERR_ARG = -1,      /* bad pointer, size or enum */
+    WT_ERR_DIMS = -2,     /* grid shape not supported (see wt_check_dims) */
+    WT_ERR_CUDA = -3,     /* a CUDA runtime call failed */
+    WT_ERR_CAPACITY = -4, /* a caller buffer is too small */
+    WT_ERR_TIMEOUT = -5   /* a bounded device wait gave up */
+};
+
+enum { WT_F32 = 0, WT_F16 = 1, WT_BF16 = 2, WT_F64 = 3 };
+
+/* wt_step flags */
+#define WT_STEP_MAC_ALL_LAST 1 /* write mac for every cell on the last step (needed before frames) */
+
+/* One tunnel's device state. Mirrors the buffers the reference Solver allocates
+ * (server/lbm.py:404-407) plus the derived per-cell code byte. */
+typedef struct wt_grid {
+    int32_t nx, ny, nz;    /* lattice size */
+    int32_t precision;     /* WT_F32 / WT_F16 / WT_BF16 / WT_F64 */
+    void* f[2];            /* two population buffers, 19*n elements each */
+    void* mac[2];          /* two macroscopic buffers, 4*n reals each (double-buffered) */
+    const uint8_t* solid;  /* n bytes, reference mask semantics */
+    uint8_t* code;         /* n bytes, filled by wt_build_codes from solid */
+} wt_grid;
+
+/* ---- library ---- */
+const char* wt_last_error(void);
+int wt_abi_version(void);
+/* 0 if (nx, ny, nz) is supported: nx even and >= 4, ny and nz >= 3, n < 2^31. */
+int wt_check_dims(int32_t nx, int32_t ny, int32_t nz);
+/* Bytes of device memory one population buffer needs at this precision. */
+int64_t wt_population_bytes(int32_t precision, int64_t n);
+
+/* ---- set-up ---- */
+/* init_kernel (server/lbm.py:64-69), launched by Solver.reset (:415-417): equilibrium at
+ * rho = 1, u = (uin, 0, 0) into population buffer f, and mac = (uin, 0, 0, 1). */
+int wt_init_eq(int32_t precision, void* f, void* mac, int64_t n, double uin, void* stream);
+/* Derive the per-cell code byte from solid (after Solver.set_solid, server/lbm.py:419-421). */
+int wt_build_codes(const wt_grid* g, void* stream);
+/* Compacted momentum-exchange link list: every interior fluid cell with at least one
+ * neighbour x + c_i whose solid byte is 1 (the cells force_kernel visits,
+ * server/lbm.py:177-193), in increasing idx order, with an 18-bit mask of those links.
+ * Two calls: wt_links_scan fills scratch (>= wt_links_scratch_len(n) int64) and writes
+ * the link count to *count_dev (device); wt_links_fill then writes cells/masks
+ * (capacity >= count). */
+int64_t wt_links_scratch_len(int64_t n);
+int wt_links_scan(const wt_grid* g, int64_t* scratch, int64_t* count_dev, void* stream);
+int wt_links_fill(const wt_grid* g, const int64_t* scratch, int32_t* cells, uint32_t* masks, int64_t capacity,
+                  void* stream);
+
+/* ---- hot path ---- */
+/* `steps` launches of step_kernel (server/lbm.py:72-166), issued by Solver.step
+ * (:442-447): fused pull-streaming, bounce-back / moving belt, equilibrium faces,
+ * regularized collision with Smagorinsky eddy viscosity and the outlet sponge. Reads
+ * f[cur], writes f[cur ^ 1], alternating; the final populations are in f[cur ^ (steps & 1)].
+ * Face cells see exactly the neighbour values the reference's serial (Warp CPU) order
+ * gives. Each step is two kernels. */
+int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
+            void* stream);
+
+/* Momentum-exchange force (force_kernel, server/lbm.py:169-197, run by Solver.frame
+ * :479-481) on f[cur] over the compacted link list. out6 (device, 6 doubles):
+ * [Fx, Fy, Fz] over all solid==1 links, then the same without links into the y = 0 plane.
+ * Per-cell sums are formed as the reference forms them; cells are accumulated in double
+ * in a fixed order (deterministic). partials: scratch of >= wt_reduce_scratch_len(n_links)
+ * doubles. */
+int64_t wt_reduce_scratch_len(int64_t count);
+int wt_forces(const wt_grid* g, int32_t cur, const int32_t* cells, const uint32_t* masks, int64_t n_links,
+              double* partials, double* out6, void* stream);
+/* Total mass sum_{fluid cells} sum_i f_i of f[cur] in double, deterministic. */
+int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void* stream);
+
+/* ---- frame outputs (Solver.frame, server/lbm.py:458-482) ---- */
+/* advect_kernel (server/lbm.py:233-263): RK2 streamline particles through mac.
+ * Respawn uses this library's counter-based RNG (not Warp's). mac: float (4*n). */
+int wt_advect(float* pos, float* spd, const float* mac, const uint8_t* solid, int32_t nx, int32_t ny, int32_t nz,
+              int64_t num_p, float dt, float uin, float max_age, uint32_t seed, float seed_x, float seed_cy,
+              float seed_cz, float seed_hy, float seed_hz, void* stream);
+/* pack_particles (server/lbm.py:266-275). */
+int wt_pack_particles(const float* pos, const float* spd, uint16_t* q16, uint8_t* q8, int32_t nx, int32_t ny,
+                      int32_t nz, int64_t num_p, void* stream);
+/* slice_kernel + vort (server/lbm.py:278-318); out has 2*w*h bytes, (w, h) per
+ * Solver.slice_dims (server/lbm.py:455-456). */
+int wt_slice(const float* mac, const uint8_t* solid, uint8_t* out, int32_t nx, int32_t ny, int32_t nz,
+             int32_t axis, int32_t index, int32_t field, float uin, float lref, float vmin, float vmax,
+             void* stream);
+/* cp_kernel + rho_fluid (server/lbm.py:321-368). verts/norms: 3 floats per vertex. */
+int wt_cp(const float* mac, const uint8_t* solid, const float* verts, const float* norms, int8_t* out, int32_t nx,
+          int32_t ny, int32_t nz, int64_t num_verts, float uin, float cp_range, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WT_H */

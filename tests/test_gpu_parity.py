@@ -1,0 +1,203 @@
+"""CUDA kernels (through libwt.so's C ABI, driven by the drop-in Solver) against the
+golden vectors of the reference's own kernels and against the pinned oracle.
+
+Tolerance: bit-exact. The library is built without FMA contraction and uses IEEE
+division and square root, and every kernel keeps the reference's association order, so
+float32 and float64 results must equal the reference's serial results exactly; fp16/bf16
+storage must equal the oracle's emulation of the same rounding exactly. The fp64 force
+and mass reductions sum in a different (fixed) order than the oracle, so they are
+compared at a relative 1e-12.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+RANDOM_CASES = ['random_12x8x10', 'random_4x4x4', 'random_28x6x5']
+TAGS = {'f32': ('fp32', np.float32, torch.float32), 'f64': ('fp64', np.float64, torch.float64)}
+
+
+def _solver(g, precision, **kw):
+    from lbm import Solver
+    s = Solver(tuple(int(v) for v in g['dims']), 'cuda:0', precision=precision, **kw)
+    s.set_solid(g['solid'])
+    return s
+
+
+def _load(s, which, arr):
+    s.f[which].copy_(torch.from_numpy(np.ascontiguousarray(arr)).to(s.f[which].dtype))
+
+
+@pytest.mark.parametrize('case', RANDOM_CASES)
+@pytest.mark.parametrize('tag', ['f32', 'f64'])
+def test_step_random_state_matches_reference(case, tag):
+    g = golden(f'{case}_{tag}.npz')
+    prec, nd, td = TAGS[tag]
+    s = _solver(g, prec)
+    _load(s, 0, g['f0_in'])
+    _load(s, 1, g['f1_in'])
+    s.mac[0].copy_(torch.from_numpy(g['mac_in']))
+    s.synchronize()
+    p = dict(uIn=float(g['uin']), tau=float(g['tau']), smag=float(g['smag']))
+    done = 0
+    for k in g['steps']:
+        s.step(int(k) - done, p)
+        done = int(k)
+        s.synchronize()
+        f_cur = s.f[s.cur].cpu().numpy()
+        f_old = s.f[1 - s.cur].cpu().numpy()
+        mac = s.mac[s.cur].cpu().numpy()
+        assert np.array_equal(f_cur, g[f'f_cur_{k}']), f'f after {k} steps: max diff {np.abs(f_cur - g[f"f_cur_{k}"]).max()}'
+        assert np.array_equal(f_old, g[f'f_old_{k}'])
+        assert np.array_equal(mac, g[f'mac_{k}'])
+        f6 = s.forces6()
+        np.testing.assert_allclose(f6[:3], g[f'forces_{k}'].astype(np.float64), rtol=2e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize('tag', ['f32', 'f64'])
+def test_sphere_100_steps_matches_reference(tag, oracle_mod):
+    g = golden(f'sphere_32x16x16_{tag}.npz')
+    prec, nd, td = TAGS[tag]
+    s = _solver(g, prec)
+    p = dict(uIn=float(g['uin']), tau=float(g['tau']), smag=float(g['smag']))
+    s.reset(p['uIn'])
+    s.step(50, p)
+    s.synchronize()
+    assert np.array_equal(s.f[s.cur].cpu().numpy(), g['f_cur_50'])
+    s.step(50, p)
+    s.synchronize()
+    assert np.array_equal(s.f[s.cur].cpu().numpy(), g['f_cur'])
+    assert np.array_equal(s.f[1 - s.cur].cpu().numpy(), g['f_old'])
+    assert np.array_equal(s.mac[s.cur].cpu().numpy(), g['mac'])
+    # forces: the reference's float sum (tid order) to float rounding; the oracle's fp64 sum
+    # of the same per-cell values to 1e-12
+    L = oracle_mod.Lattice(tuple(int(v) for v in g['dims']), oracle_mod.F32 if tag == 'f32' else oracle_mod.F64)
+    L.solid[:] = g['solid']
+    L.f[0][:] = g['f_cur']
+    _, d64, b64 = L.forces()
+    f6 = s.forces6()
+    np.testing.assert_allclose(f6[:3], d64, rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(f6[3:], b64, rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(f6[:3], g['forces'].astype(np.float64), rtol=2e-5, atol=1e-7)
+    np.testing.assert_allclose(s.mass(), L.mass(), rtol=1e-13)
+
+
+def test_frame_kernels_match_reference():
+    g = golden('sphere_32x16x16_f32.npz')
+    s = _solver(g, 'fp32')
+    dims = tuple(int(v) for v in g['dims'])
+    s.mac[s.cur].copy_(torch.from_numpy(g['mac']))
+    dt, uin, max_age, seed, sx, scy, scz, shy, shz = (float(v) for v in g['adv_params'])
+    # particles: place the golden inputs, advect once with the golden seed
+    s.num_p = len(g['adv_pos_in'])
+    s.pos = torch.from_numpy(g['adv_pos_in'].copy()).cuda()
+    s.spd = torch.ones(s.num_p, dtype=torch.float32, device='cuda')
+    s.q16 = torch.zeros(s.num_p * 4, dtype=torch.int16, device='cuda')
+    s.q8 = torch.zeros(s.num_p, dtype=torch.uint8, device='cuda')
+    s.synchronize()
+    s.seed = int(seed) - 1
+    p = dict(uIn=uin, tau=0.506, smag=0.16, maxAge=max_age, seedX=sx, seedCy=scy, seedCz=scz, seedHy=shy,
+             seedHz=shz, lref=8.0)
+    s.seed += 1
+    s._advect(dt, p)
+    s.synchronize()
+    assert np.array_equal(s.pos.cpu().numpy(), g['adv_pos'])
+    assert np.array_equal(s.spd.cpu().numpy(), g['adv_spd'])
+    s.set_surface(g['cp_verts'], g['cp_norms'])
+    for axis in (0, 1, 2):
+        for field in range(4):
+            a = g[f'slice_{axis}_{field}_args']
+            p['slice'] = dict(axis=int(a[0]), index=int(a[1]), field=int(a[2]), vmin=float(a[4]), vmax=float(a[5]))
+            p['lref'] = float(a[3])
+            out = s.frame(p, want_cp=True)
+            assert np.array_equal(out['slice'], g[f'slice_{axis}_{field}']), (axis, field)
+            assert (out['sliceW'], out['sliceH'], out['sliceAxis']) == s.slice_dims(axis) + (axis,)
+    assert np.array_equal(out['parts16'], g['pack_q16'])
+    assert np.array_equal(out['parts8'], g['pack_q8'])
+    assert np.array_equal(out['cp'], g['cp'])
+    assert len(out['forces']) == 3
+
+
+def _random_case(dims, seed, belt=True):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    r = rng.random(n)
+    solid = np.zeros(n, np.uint8)
+    solid[r < 0.08] = 1
+    solid[(r > 0.5) & (r < 0.52)] = 2
+    if belt:
+        solid.reshape(nz, ny, nx)[:, 0, :] = 2
+    return solid
+
+
+@pytest.mark.parametrize('prec_name,oprec', [('fp32', 0), ('fp16', 1), ('bf16', 2), ('fp64', 3)])
+@pytest.mark.parametrize('dims', [(64, 24, 20), (34, 9, 7)])
+def test_random_obstacles_match_oracle(oracle_mod, prec_name, oprec, dims):
+    """Larger grids than the goldens, every storage precision, against the pinned oracle."""
+    solid = _random_case(dims, 5)
+    uin, tau, smag = 0.06, 0.52, 0.16
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name)
+    s.reset(uin)
+    L = oracle_mod.Lattice(dims, oprec)
+    L.solid[:] = solid
+    L.reset(uin)
+    p = dict(uIn=uin, tau=tau, smag=smag)
+    for chunk in (1, 4, 7):
+        s.step(chunk, p)
+        L.step(chunk, uin, tau, smag)
+        s.synchronize()
+        dev = s.f[s.cur].cpu()
+        if oprec == 2:
+            dev = dev.view(torch.int16).numpy().view(np.uint16)
+        else:
+            dev = dev.numpy()
+        assert np.array_equal(dev, L.f[L.cur]), f'{prec_name} after chunk {chunk}'
+        assert np.array_equal(s.mac[s.cur].cpu().numpy(), L.mac)
+    _, d64, b64 = L.forces()
+    f6 = s.forces6()
+    np.testing.assert_allclose(f6[:3], d64, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(f6[3:], b64, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(s.mass(), L.mass(), rtol=1e-13)
+
+
+def test_link_list_matches_mask():
+    dims = (48, 20, 18)
+    solid = _random_case(dims, 9)
+    s = _solver(dict(dims=np.array(dims), solid=solid), 'fp32')
+    nx, ny, nz = dims
+    from bodies import C
+    expect_cells, expect_masks = [], []
+    v = solid.reshape(nz, ny, nx)
+    for z in range(1, nz - 1):
+        for y in range(1, ny - 1):
+            for x in range(1, nx - 1):
+                if v[z, y, x]:
+                    continue
+                m = 0
+                for i in range(1, 19):
+                    if v[z + C[i][2], y + C[i][1], x + C[i][0]] == 1:
+                        m |= 1 << (i - 1)
+                if m:
+                    expect_cells.append(x + nx * (y + ny * z))
+                    expect_masks.append(m)
+    assert s.n_links == len(expect_cells)
+    assert np.array_equal(s.link_cells[:s.n_links].cpu().numpy(), np.array(expect_cells, np.int32))
+    assert np.array_equal(s.link_masks[:s.n_links].cpu().numpy().view(np.uint32), np.array(expect_masks, np.uint32))
+
+
+def test_repeatable_bitwise():
+    dims = (64, 24, 20)
+    solid = _random_case(dims, 3)
+    outs = []
+    for _ in range(2):
+        s = _solver(dict(dims=np.array(dims), solid=solid), 'fp32')
+        s.reset(0.05)
+        s.step(20, dict(uIn=0.05, tau=0.51, smag=0.16))
+        outs.append((s.f[s.cur].cpu().numpy(), s.forces6(), s.mass()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]

@@ -1,0 +1,289 @@
+"""B200 lattice-Boltzmann wind tunnel (D3Q19, regularized collision + Smagorinsky LES).
+
+Drop-in replacement for the reference's ``server/lbm.py`` (RICKxxROLLING/wind-tunnel):
+the same module exports (``RESOLUTIONS``, ``BYTES_PER_CELL``, ``Solver``) and the same
+``Solver`` methods and attributes that ``server/app.py`` drives
+(``server/lbm.py:398-482``). The work runs in hand-written sm_100a kernels in
+``libwt.so`` called through the C ABI of ``include/wt.h``; torch tensors serve only as
+device buffers. There is no CPU path: constructing a Solver without a CUDA device raises.
+
+Lattice frame as in the reference: x streamwise (flow +x), y vertical, z span; cell
+centres at integer coordinates; cell index ``idx = x + nx * (y + ny * z)``.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+import wtlib as W
+from wtlib import call, ptr
+
+Q = 19
+
+# grid presets (server/lbm.py:21-29)
+RESOLUTIONS = {
+    'test': (64, 28, 36),
+    'low': (128, 56, 72),
+    'medium': (176, 80, 96),
+    'high': (256, 112, 136),
+    'ultra': (352, 144, 176),
+    'extreme': (448, 192, 224),
+    'max': (544, 224, 272),
+}
+
+CP_RANGE = 1.2  # server/lbm.py:395
+
+_POP_BYTES = {W.F32: 4, W.F16: 2, W.F64: 8, W.BF16: 2}
+_TORCH_POP = {W.F32: torch.float32, W.F16: torch.float16, W.BF16: torch.bfloat16, W.F64: torch.float64}
+
+
+def bytes_per_cell(precision='fp32'):
+    """Device bytes per cell: two population buffers, two mac buffers, solid and code bytes."""
+    prec = W.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    mac = 32 if prec == W.F64 else 16
+    return 2 * Q * _POP_BYTES[prec] + 2 * mac + 2
+
+
+# The reference's name for the admission footprint (server/lbm.py:30, used by app.py:76).
+BYTES_PER_CELL = bytes_per_cell('fp32')
+
+
+def _device(device):
+    if not torch.cuda.is_available():
+        raise RuntimeError('wind-tunnel_b200 needs a CUDA device; there is no CPU path')
+    if device is None:
+        return torch.device('cuda', torch.cuda.current_device())
+    if isinstance(device, int):
+        return torch.device('cuda', device)
+    d = torch.device(device)
+    if d.type != 'cuda':
+        raise RuntimeError(f'device {device!r} is not a CUDA device; there is no CPU path')
+    return d if d.index is not None else torch.device('cuda', torch.cuda.current_device())
+
+
+class Solver:
+    """One tunnel. Method-for-method the reference Solver (server/lbm.py:398-482).
+
+    Extra keyword arguments: ``precision`` ('fp32' as the reference, 'fp16'/'bf16' for
+    shifted half-width population storage, 'fp64' for the oracle run), ``stream`` (a
+    ``torch.cuda.Stream``; by default each Solver owns one) and ``seed`` (particle
+    initialisation; the reference draws from an unseeded generator).
+    """
+
+    def __init__(self, dims, device=None, precision='fp32', stream=None, seed=None):
+        self.dev = _device(device)
+        self.nx, self.ny, self.nz = (int(d) for d in dims)
+        self.n = n = self.nx * self.ny * self.nz
+        call('wt_check_dims', self.nx, self.ny, self.nz)
+        self.precision = W.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        if self.precision not in _TORCH_POP:
+            raise ValueError(f'unknown precision {precision!r}')
+        self.stream = stream if stream is not None else torch.cuda.Stream(self.dev)
+        mac_dt = torch.float64 if self.precision == W.F64 else torch.float32
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            # zero-filled like the reference's wp.zeros buffers (server/lbm.py:404-407)
+            self.f = [torch.zeros(Q * n, dtype=_TORCH_POP[self.precision], device=self.dev) for _ in range(2)]
+            self.mac = [torch.zeros((n, 4), dtype=mac_dt, device=self.dev) for _ in range(2)]
+            self.solid = torch.zeros(n, dtype=torch.uint8, device=self.dev)
+            self.code = torch.zeros(n, dtype=torch.uint8, device=self.dev)
+            self.forces_dev = torch.zeros(6, dtype=torch.float64, device=self.dev)
+            self.mass_dev = torch.zeros(1, dtype=torch.float64, device=self.dev)
+            self.partials = torch.empty(int(W.lib().wt_reduce_scratch_len(0)), dtype=torch.float64, device=self.dev)
+            self.slice_max = max(self.nx * self.ny, self.nx * self.nz, self.nz * self.ny)
+            self.slice_buf = torch.zeros(self.slice_max * 2, dtype=torch.uint8, device=self.dev)
+            self.link_cells = torch.zeros(0, dtype=torch.int32, device=self.dev)
+            self.link_masks = torch.zeros(0, dtype=torch.int32, device=self.dev)
+        self.n_links = 0
+        self.grid = W.Grid(self.nx, self.ny, self.nz, self.precision,
+                           (ctypes.c_void_p * 2)(self.f[0].data_ptr(), self.f[1].data_ptr()),
+                           (ctypes.c_void_p * 2)(self.mac[0].data_ptr(), self.mac[1].data_ptr()),
+                           self.solid.data_ptr(), self.code.data_ptr())
+        self.gp = ctypes.byref(self.grid)
+        self.sh = W.stream_handle(self.stream)
+        self.cur = 0
+        self.num_p = 0
+        self.num_verts = 0
+        self.seed = 1
+        self.rng = np.random.default_rng(seed)
+        self._host = {}
+        self._pending = None
+        self.stream.synchronize()
+
+    # ---- set-up (server/lbm.py:415-440) ----
+    def reset(self, uin):
+        """Equilibrium at rho = 1, u = (uin, 0, 0) in both population buffers (init_kernel)."""
+        for b in range(2):
+            call('wt_init_eq', self.precision, ptr(self.f[b]), ptr(self.mac[b]), self.n, float(uin), self.sh)
+
+    def set_solid(self, arr):
+        """Upload the voxel mask (0 fluid, 1 solid, 2 moving belt) and rebuild the per-cell
+        codes and the compacted momentum-exchange link list."""
+        arr = np.asarray(arr)
+        assert arr.size == self.n
+        host = torch.from_numpy(np.ascontiguousarray(arr.reshape(-1).astype(np.uint8)))
+        with torch.cuda.stream(self.stream):
+            self.solid.copy_(host.pin_memory(), non_blocking=True)
+            call('wt_build_codes', self.gp, self.sh)
+            scratch = torch.empty(int(W.lib().wt_links_scratch_len(self.n)), dtype=torch.int64, device=self.dev)
+            count = torch.zeros(1, dtype=torch.int64, device=self.dev)
+            call('wt_links_scan', self.gp, ptr(scratch), ptr(count), self.sh)
+            self.n_links = int(count.to('cpu', non_blocking=False).item())
+            cap = max(1, self.n_links)
+            self.link_cells = torch.empty(cap, dtype=torch.int32, device=self.dev)
+            self.link_masks = torch.empty(cap, dtype=torch.int32, device=self.dev)
+            call('wt_links_fill', self.gp, ptr(scratch), ptr(self.link_cells), ptr(self.link_masks), cap, self.sh)
+        self.stream.synchronize()
+
+    def set_surface(self, verts, norms):
+        verts = np.ascontiguousarray(np.asarray(verts, np.float32).reshape(-1, 3))
+        norms = np.ascontiguousarray(np.asarray(norms, np.float32).reshape(-1, 3))
+        self.num_verts = len(verts)
+        with torch.cuda.stream(self.stream):
+            self.verts = torch.from_numpy(verts).to(self.dev, non_blocking=False)
+            self.norms = torch.from_numpy(norms).to(self.dev, non_blocking=False)
+            self.cp_buf = torch.zeros(max(1, self.num_verts), dtype=torch.int8, device=self.dev)
+
+    def set_particles(self, count, p):
+        """Streamline particles in the rake box (server/lbm.py:429-440), from this Solver's
+        seeded generator."""
+        rng = self.rng
+        d = np.zeros((count, 4), np.float32)
+        d[:, 0] = 2 + rng.random(count) * (self.nx - 8)
+        d[:, 1] = p['seedCy'] + (rng.random(count) * 2 - 1) * p['seedHy']
+        d[:, 2] = p['seedCz'] + (rng.random(count) * 2 - 1) * p['seedHz']
+        d[:, 3] = rng.random(count) * p['maxAge'] * 0.5
+        self.num_p = count
+        with torch.cuda.stream(self.stream):
+            self.pos = torch.from_numpy(d).to(self.dev)
+            self.spd = torch.ones(count, dtype=torch.float32, device=self.dev)
+            self.q16 = torch.zeros(count * 4, dtype=torch.int16, device=self.dev)
+            self.q8 = torch.zeros(count, dtype=torch.uint8, device=self.dev)
+        self.stream.synchronize()
+
+    # ---- hot path (server/lbm.py:442-453) ----
+    def step(self, steps, p):
+        steps = int(steps)
+        if steps > 0:
+            call('wt_step', self.gp, self.cur, steps, float(p['uIn']), float(p['tau']), float(p['smag']),
+                 W.STEP_MAC_ALL_LAST, self.sh)
+            self.cur ^= steps & 1
+        if self.num_p and steps:
+            self.seed += 1
+            self._advect(float(steps), p)
+
+    def _advect(self, dt, p):
+        self._require_float_mac('particles')
+        call('wt_advect', ptr(self.pos), ptr(self.spd), ptr(self.mac[self.cur]), ptr(self.solid), self.nx, self.ny,
+             self.nz, self.num_p, dt, float(p['uIn']), float(p['maxAge']), self.seed & 0xFFFFFFFF,
+             float(p['seedX']), float(p['seedCy']), float(p['seedCz']), float(p['seedHy']), float(p['seedHz']),
+             self.sh)
+
+    def slice_dims(self, axis):
+        return {2: (self.nx, self.ny), 1: (self.nx, self.nz), 0: (self.nz, self.ny)}[axis]
+
+    # ---- frame outputs (server/lbm.py:458-482) ----
+    def _pinned(self, key, shape, dtype):
+        t = self._host.get(key)
+        if t is None or t.shape != torch.Size(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, pin_memory=True)
+            self._host[key] = t
+        return t
+
+    def _require_float_mac(self, what):
+        if self.precision == W.F64:
+            raise NotImplementedError(f'{what} output needs float mac; the fp64 run reports forces and mass only')
+
+    def launch_frame(self, p, want_cp, copy=True):
+        """Queue every frame kernel and (with copy) its device-to-host copy on the Solver's
+        stream without waiting; collect_frame() waits once and returns the reference's dict."""
+        out = {}
+        copies = []
+        mac = self.mac[self.cur]
+        if self.num_p:
+            self._require_float_mac('particles')
+            call('wt_pack_particles', ptr(self.pos), ptr(self.spd), ptr(self.q16), ptr(self.q8), self.nx, self.ny,
+                 self.nz, self.num_p, self.sh)
+            copies.append(('parts16', self.q16, self._pinned('q16', (self.num_p * 4,), torch.int16)))
+            copies.append(('parts8', self.q8, self._pinned('q8', (self.num_p,), torch.uint8)))
+        sl = p.get('slice')
+        if sl and sl.get('field', -1) >= 0:
+            self._require_float_mac('slice')
+            axis = int(sl['axis'])
+            w, h = self.slice_dims(axis)
+            dim = (self.nx, self.ny, self.nz)[axis]
+            index = max(0, min(dim - 1, int(sl['index'])))
+            call('wt_slice', ptr(mac), ptr(self.solid), ptr(self.slice_buf), self.nx, self.ny, self.nz, axis, index,
+                 int(sl['field']), float(p['uIn']), float(p['lref']), float(sl['vmin']), float(sl['vmax']), self.sh)
+            copies.append(('slice', self.slice_buf[:w * h * 2], self._pinned('slice', (w * h * 2,), torch.uint8)))
+            out['sliceW'], out['sliceH'], out['sliceAxis'] = w, h, axis
+        if want_cp and self.num_verts:
+            self._require_float_mac('surface pressure')
+            call('wt_cp', ptr(mac), ptr(self.solid), ptr(self.verts), ptr(self.norms), ptr(self.cp_buf), self.nx,
+                 self.ny, self.nz, self.num_verts, float(p['uIn']), CP_RANGE, self.sh)
+            copies.append(('cp', self.cp_buf[:self.num_verts], self._pinned('cp', (self.num_verts,), torch.int8)))
+        call('wt_forces', self.gp, self.cur, ptr(self.link_cells), ptr(self.link_masks), self.n_links,
+             ptr(self.partials), ptr(self.forces_dev), self.sh)
+        copies.append(('forces6', self.forces_dev, self._pinned('forces6', (6,), torch.float64)))
+        if not copy:
+            self._pending = None
+            return
+        with torch.cuda.stream(self.stream):
+            for _, src, dst in copies:
+                dst.copy_(src, non_blocking=True)
+        self._pending = (out, copies)
+
+    def collect_frame(self):
+        out, copies = self._pending
+        self._pending = None
+        self.stream.synchronize()
+        views = {'parts16': np.uint16, 'parts8': np.uint8, 'slice': np.uint8, 'cp': np.int8}
+        for key, _, dst in copies:
+            a = dst.numpy()
+            if key == 'forces6':
+                self.last_forces6 = a.copy()
+                out['forces'] = [float(v) for v in a[:3]]
+            else:
+                out[key] = a.view(views[key]).copy()
+        return out
+
+    def frame(self, p, want_cp):
+        """Reference Solver.frame: particles, slice, surface Cp and forces in one dict."""
+        self.launch_frame(p, want_cp)
+        return self.collect_frame()
+
+    # ---- extras used by tests, the serving loop and the benchmark ----
+    def forces6(self):
+        """[Fx, Fy, Fz] over all solid==1 links, then without links into the y = 0 plane (fp64)."""
+        call('wt_forces', self.gp, self.cur, ptr(self.link_cells), ptr(self.link_masks), self.n_links,
+             ptr(self.partials), ptr(self.forces_dev), self.sh)
+        self.stream.synchronize()
+        return self.forces_dev.cpu().numpy().copy()
+
+    def mass(self):
+        call('wt_mass', self.gp, self.cur, ptr(self.partials), ptr(self.mass_dev), self.sh)
+        self.stream.synchronize()
+        return float(self.mass_dev.cpu()[0])
+
+    def populations(self, which=None):
+        """Populations of buffer ``which`` (default current) as float64 numpy (19, n),
+        with the w_i shift of fp16/bf16 storage removed."""
+        self.stream.synchronize()
+        f = self.f[self.cur if which is None else which].double().cpu().numpy().reshape(Q, self.n)
+        if self.precision in (W.F16, W.BF16):
+            f = f + np.array(_weights())[:, None]
+        return f
+
+    def macro(self):
+        """mac of the current buffer as float64 numpy (n, 4): ux, uy, uz, rho."""
+        self.stream.synchronize()
+        return self.mac[self.cur].double().cpu().numpy()
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+
+def _weights():
+    c = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
+         (1, 1, 0), (-1, -1, 0), (1, -1, 0), (-1, 1, 0), (1, 0, 1), (-1, 0, -1), (1, 0, -1), (-1, 0, 1),
+         (0, 1, 1), (0, -1, -1), (0, 1, -1), (0, -1, 1)]
+    return [1 / 3 if i == 0 else (1 / 18 if sum(map(abs, v)) == 1 else 1 / 36) for i, v in enumerate(c)]
