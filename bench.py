@@ -158,11 +158,17 @@ def run_ours(args, rank, world, local_rank):
         return float(t.item())
 
     # ---- device-resident frame loop ----
-    s = lbm.Solver(dims, dev, precision=prec, seed=1234 + rank)
+    s = lbm.Solver(dims, dev, precision=prec, seed=1234 + rank, collision=args.collision)
     s.set_solid(solid)
     s.set_surface(verts, norms)
     s.reset(p['uIn'])
     s.set_particles(N_PARTICLES, p)
+    import autotune
+    if args.tile:
+        tile, tile_ms = args.tile, {}
+        s.set_tile(tile)
+    else:
+        tile, tile_ms = autotune.tune(s, p, force=True)  # part of the warm-up
     launches_per_frame = 2 * STEPS_PER_FRAME + 1 + 1 + 1 + 1 + 2  # steps, advect, pack, slice, cp, forces(2)
 
     def frame_device():
@@ -201,7 +207,8 @@ def run_ours(args, rank, world, local_rank):
                 'peak_source': f'{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)' if peak_kind == 'measured'
                 else 'fallback 6.65 TB/s', 'kernel': f'wt_step ({prec}) = k_step_bulk + k_step_faces, one LBM step',
                 'algorithmic_bytes_per_cell': ALGO_BYTES[prec], 'step_ms': round(t_step * 1e3, 4),
-                'glups_step_only': round(n / t_step / 1e9, 3)}
+                'glups_step_only': round(n / t_step / 1e9, 3), 'tile': tile,
+                'tile_ms_per_step': {str(k): round(v, 4) for k, v in tile_ms.items()}}
     del s
     torch.cuda.empty_cache()
 
@@ -213,7 +220,8 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    s = lbm.Solver(dims, dev, precision=prec, seed=99 + rank)
+    s = lbm.Solver(dims, dev, precision=prec, seed=99 + rank, collision=args.collision)
+    s.set_tile(tile)
     s.set_solid(host_solid)
     s.set_surface(host_verts, host_norms)
     s.reset(p['uIn'])
@@ -237,13 +245,14 @@ def run_ours(args, rank, world, local_rank):
     del s
     torch.cuda.empty_cache()
 
-    # ---- storage-precision variants of the step (same workload) ----
+    # ---- storage-precision / collision-form variants of the step (same workload) ----
     variants = {}
     if args.variants and prec == 'fp32':
-        for vp in ('fp16', 'bf16'):
-            v = lbm.Solver(dims, dev, precision=vp)
+        for vp, vc in (('fp32', 'fast'), ('fp16', 'fast'), ('bf16', 'fast'), ('fp16', 'exact')):
+            v = lbm.Solver(dims, dev, precision=vp, collision=vc)
             v.set_solid(solid)
             v.reset(p['uIn'])
+            vtile, vms = autotune.tune(v, p, force=True)
             v.step(5, p)
             torch.cuda.synchronize(dev)
             ev0.record(v.stream)
@@ -251,13 +260,19 @@ def run_ours(args, rank, world, local_rank):
             ev1.record(v.stream)
             torch.cuda.synchronize(dev)
             tv = ev0.elapsed_time(ev1) / 1e3 / nstep
-            variants[vp] = {'glups_step_only': round(n / tv / 1e9, 3),
+            variants[f'{vp}-{vc}'] = {'glups_step_only': round(n / tv / 1e9, 3),
                             'achieved_gbs': round(ALGO_BYTES[vp] * n / tv / 1e9, 1),
-                            'speedup_vs_fp32_step': round(t_step / tv, 3)}
+                            'speedup_vs_fp32_step': round(t_step / tv, 3), 'tile': vtile,
+                            'tile_ms_per_step': {str(k): round(x, 4) for k, x in vms.items()}}
             del v
             torch.cuda.empty_cache()
 
-    return dict(value=value, t_dev=t_dev, roofline=roofline, e2e=e2e, clocks=clk.summary(),
+    acc = None
+    if args.accuracy and prec == 'fp32' and rank == 0:
+        import accuracy
+        acc = accuracy.study(steps=args.accuracy_steps, scale=0.5, device=dev)
+
+    return dict(value=value, t_dev=t_dev, roofline=roofline, e2e=e2e, clocks=clk.summary(), accuracy=acc,
                 launches=launches_per_frame * args.steps, dims=dims, n=n, variants=variants)
 
 
@@ -292,10 +307,15 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp16', 'bf16', 'fp64'])
+    ap.add_argument('--collision', default=None, choices=['exact', 'fast'],
+                    help='collision form (default: exact for fp32/fp64, fast for fp16/bf16)')
+    ap.add_argument('--tile', type=int, default=0, help='step tile variant (0 = autotune)')
     ap.add_argument('--scale', type=float, default=1.0, help='grid scale (1.0 = 512x256x256)')
     ap.add_argument('--cpu-budget', type=float, default=12.0)
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-variants', dest='variants', action='store_false')
+    ap.add_argument('--no-accuracy', dest='accuracy', action='store_false')
+    ap.add_argument('--accuracy-steps', type=int, default=2000)
     args = ap.parse_args()
 
     world = env_int('WORLD_SIZE', 1)
@@ -335,7 +355,7 @@ def main():
                    'cells': r['n'], 'steps_per_frame': STEPS_PER_FRAME, 'l2': 'inputs larger than L2 (no flush)',
                    'parallelism': f'replicas x{world}'},
         'roofline': r['roofline'], 'cpu_baseline': cpu, 'e2e': r['e2e'], 'clocks': r['clocks'],
-        'gpu_launches': r['launches'], 'precision_variants': r['variants'],
+        'gpu_launches': r['launches'], 'precision_variants': r['variants'], 'accuracy_vs_fp64': r['accuracy'],
     }
     print(json.dumps(line), flush=True)
 

@@ -44,6 +44,13 @@ enum {
 
 enum { WT_F32 = 0, WT_F16 = 1, WT_BF16 = 2, WT_F64 = 3 };
 
+/* collision forms. EXACT evaluates the reference's expressions in the reference's order
+ * (bit-identical to server/lbm.py run serially). FAST evaluates the same regularized
+ * Smagorinsky collision in moment space with fused multiply-adds (about 40% fewer
+ * operations; equal to EXACT up to rounding); with fp16/bf16 storage it works on the
+ * stored deviations f_i - w_i directly. */
+enum { WT_COLLIDE_EXACT = 0, WT_COLLIDE_FAST = 1 };
+
 /* wt_step flags */
 #define WT_STEP_MAC_ALL_LAST 1 /* write mac for every cell on the last step (needed before frames) */
 
@@ -56,6 +63,12 @@ typedef struct wt_grid {
     void* mac[2];          /* two macroscopic buffers, 4*n reals each (double-buffered) */
     const uint8_t* solid;  /* n bytes, reference mask semantics */
     uint8_t* code;         /* n bytes, filled by wt_build_codes from solid */
+    int32_t tile;          /* step kernel tile variant (wt_step_tiles); 0 = library default */
+    int32_t collision;     /* WT_COLLIDE_EXACT (reference operation order) or WT_COLLIDE_FAST */
+    int32_t* status;       /* optional device int: set to WT_ERR_TIMEOUT if a bounded wait gives up */
+    int32_t test_skip_chunk; /* test hook for the failure path: 0 = off; k > 0: chunk k-1 of a
+                                streaming tile is never loaded, so its bounded wait expires */
+    int32_t pad_;
 } wt_grid;
 
 /* ---- library ---- */
@@ -82,6 +95,12 @@ int64_t wt_links_scratch_len(int64_t n);
 int wt_links_scan(const wt_grid* g, int64_t* scratch, int64_t* count_dev, void* stream);
 int wt_links_fill(const wt_grid* g, const int64_t* scratch, int32_t* cells, uint32_t* masks, int64_t capacity,
                   void* stream);
+
+/* Tile variants of the step kernel: writes up to `cap` rows of 4 ints into out and returns
+ * the count. Direct-load tiles: {id, cells_per_thread, threads_per_block,
+ * min_blocks_per_sm}; streaming tiles (shared-memory staging through bulk async copies):
+ * {id, -chunk_cells, threads_per_block, pipeline_stages}. Select one with wt_grid.tile. */
+int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap);
 
 /* ---- hot path ---- */
 /* `steps` launches of step_kernel (server/lbm.py:72-166), issued by Solver.step

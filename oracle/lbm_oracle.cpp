@@ -90,8 +90,109 @@ inline void st(typename St::Store* f, int64_t n, int i, int64_t idx, typename St
     else f[(int64_t)i * n + idx] = (S)v;
 }
 
+// raw stored value (the fast collision works on deviations directly for shifted storage)
+template <class St>
+inline typename St::Real ldv(const typename St::Store* f, int64_t n, int i, int64_t idx) {
+    return (typename St::Real)f[(int64_t)i * n + idx];
+}
+template <class St>
+inline void stv(typename St::Store* f, int64_t n, int i, int64_t idx, typename St::Real v) {
+    f[(int64_t)i * n + idx] = (typename St::Store)v;
+}
+
 template <class T>
 inline T clampT(T x, T a, T b) { return std::min(std::max(x, a), b); }
+
+template <class T>
+inline T fmaT(T a, T b, T c) { return std::fma(a, b, c); }
+
+// Moment-space form of the regularized Smagorinsky collision: the same operation
+// sequence as collide_fast in the CUDA library (wt_step.cu), so results are bit-identical.
+// Mathematically equal to the reference collision; see the CUDA source for the derivation.
+template <class T, bool SHIFT>
+void collide_fast(T (&v)[Q], int x, int nx, T tau, T csmag, T& oux, T& ouy, T& ouz, T& orho) {
+    const double wd0 = w_d(0), wd1 = w_d(1), wd7 = w_d(7);
+    const T s1 = v[1] + v[2], a1 = v[1] - v[2];
+    const T s3 = v[3] + v[4], a3 = v[3] - v[4];
+    const T s5 = v[5] + v[6], a5 = v[5] - v[6];
+    const T s7 = v[7] + v[8], a7 = v[7] - v[8];
+    const T s9 = v[9] + v[10], a9 = v[9] - v[10];
+    const T s11 = v[11] + v[12], a11 = v[11] - v[12];
+    const T s13 = v[13] + v[14], a13 = v[13] - v[14];
+    const T s15 = v[15] + v[16], a15 = v[15] - v[16];
+    const T s17 = v[17] + v[18], a17 = v[17] - v[18];
+    const T d7 = s7 + s9, d11 = s11 + s13, d15 = s15 + s17;
+    const T xxx = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
+    const T xxy = s7 - s9, xxz = s11 - s13, xyz = s15 - s17;
+    const T S = ((v[0] + s1) + (s3 + s5)) + ((d7 + d11) + d15);
+    const T jx = ((a1 + a7) + (a9 + a11)) + a13;
+    const T jy = ((a3 + a7) - (a9 - a15)) + a17;
+    const T jz = ((a5 + a11) - (a13 - a15)) - a17;
+    const T rho = SHIFT ? S + (T)1.0 : S;
+    const T ir = (T)1.0 / rho;
+    T ux = jx * ir, uy = jy * ir, uz = jz * ir;
+    T usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
+    if (usq > (T)0.1225) {
+        const T sc = (T)0.35 / std::sqrt(usq);
+        ux = ux * sc; uy = uy * sc; uz = uz * sc;
+        usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
+    }
+    const T rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    const T t3 = (SHIFT ? S : rho) * ((T)1.0 / (T)3.0);
+    const T nxx = fmaT(-rux, ux, xxx - t3), nyy = fmaT(-ruy, uy, xyy - t3), nzz = fmaT(-ruz, uz, xzz - t3);
+    const T nxy = fmaT(-rux, uy, xxy), nxz = fmaT(-rux, uz, xxz), nyz = fmaT(-ruy, uz, xyz);
+    const T q1 = fmaT(nzz, nzz, fmaT(nyy, nyy, nxx * nxx));
+    const T q2 = fmaT(nyz, nyz, fmaT(nxz, nxz, nxy * nxy));
+    const T qn = std::sqrt(fmaT((T)2.0, q2, q1));
+    T tau0 = tau;
+    const T sp = (T)x - (T)(nx - 24);
+    if (sp > (T)0.0) tau0 = fmaT(sp, (T)0.015, tau);
+    const T tau_e = (T)0.5 * (tau0 + std::sqrt(fmaT(tau0, tau0, csmag * qn * ir)));
+    const T keep = (T)1.0 - (T)1.0 / tau_e;
+    const T k45 = (T)4.5 * keep, k9 = (T)9.0 * keep;
+    const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
+    const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;
+    const T tra3 = ((axx + ayy) + azz) * ((T)1.0 / (T)3.0);
+    const T B = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+    const T w0 = (T)wd0, w1 = (T)wd1, w2 = (T)wd7;
+    const T w1x3 = (T)(3.0 * wd1), w2x3 = (T)(3.0 * wd7);
+    v[0] = w0 * B;
+    const T bxx = B + axx, byy = B + ayy;
+    auto pair = [&](int i, T w, T wx3, T D, T rs) {
+        const T E = wx3 * rs;
+        v[i] = fmaT(w, D, E);
+        v[i + 1] = fmaT(w, D, -E);
+    };
+    pair(1, w1, w1x3, fmaT((T)4.5 * rux, ux, bxx), rux);
+    pair(3, w1, w1x3, fmaT((T)4.5 * ruy, uy, byy), ruy);
+    pair(5, w1, w1x3, fmaT((T)4.5 * ruz, uz, B + azz), ruz);
+    const T pxy = bxx + ayy, pxz = bxx + azz, pyz = byy + azz;
+    {
+        const T su = ux + uy, rs = rux + ruy;
+        pair(7, w2, w2x3, fmaT((T)4.5 * rs, su, pxy + axy), rs);
+    }
+    {
+        const T su = ux - uy, rs = rux - ruy;
+        pair(9, w2, w2x3, fmaT((T)4.5 * rs, su, pxy - axy), rs);
+    }
+    {
+        const T su = ux + uz, rs = rux + ruz;
+        pair(11, w2, w2x3, fmaT((T)4.5 * rs, su, pxz + axz), rs);
+    }
+    {
+        const T su = ux - uz, rs = rux - ruz;
+        pair(13, w2, w2x3, fmaT((T)4.5 * rs, su, pxz - axz), rs);
+    }
+    {
+        const T su = uy + uz, rs = ruy + ruz;
+        pair(15, w2, w2x3, fmaT((T)4.5 * rs, su, pyz + ayz), rs);
+    }
+    {
+        const T su = uy - uz, rs = ruy - ruz;
+        pair(17, w2, w2x3, fmaT((T)4.5 * rs, su, pyz - ayz), rs);
+    }
+    oux = ux; ouy = uy; ouz = uz; orho = rho;
+}
 inline int clampI(int x, int a, int b) { return std::min(std::max(x, a), b); }
 
 // ---------------- init (server/lbm.py:64-69) ----------------
@@ -121,6 +222,7 @@ struct StepArgs {
     int nx, ny, nz;
     int64_t n;
     T uin, tau, smag;
+    int fast;  // 1: moment-space collision (collide_fast)
 };
 
 // One cell of step_kernel. `cur_mac` is where a face cell reads its neighbour's mac.
@@ -157,6 +259,27 @@ void step_cell(const StepArgs<St>& a, int64_t idx, int x, int y, int z, const ty
             st<St>(a.fout, n, i, idx, K.w[i] * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq), K);
         }
         mac[4 * idx + 0] = bux; mac[4 * idx + 1] = buy; mac[4 * idx + 2] = buz; mac[4 * idx + 3] = br;
+        return;
+    }
+    if (a.fast) {
+        T v[Q];
+        v[0] = ldv<St>(a.fin, n, 0, idx);
+        const int64_t sy = nx, sz = (int64_t)nx * ny;
+        for (int i = 1; i < Q; ++i) {
+            int64_t s = idx - CX[i] - CY[i] * sy - CZ[i] * sz;
+            int t = a.solid[s];
+            if (t == 0) {
+                v[i] = ldv<St>(a.fin, n, i, s);
+            } else {
+                v[i] = ldv<St>(a.fin, n, OPP[i], idx);  // w_opp = w_i: deviations carry over
+                if (CX[i] != 0 && t == 2) v[i] = v[i] + K.belt[i] * a.uin;
+            }
+        }
+        T ux, uy, uz, rho;
+        const T csmag = (T)25.4558441 * a.smag * a.smag;
+        collide_fast<T, St::shifted>(v, x, nx, a.tau, csmag, ux, uy, uz, rho);
+        for (int i = 0; i < Q; ++i) stv<St>(a.fout, n, i, idx, v[i]);
+        mac[4 * idx + 0] = ux; mac[4 * idx + 1] = uy; mac[4 * idx + 2] = uz; mac[4 * idx + 3] = rho;
         return;
     }
     T f[Q];
@@ -514,8 +637,8 @@ void cp_impl(const T* mac, const uint8_t* solid, const T* verts, const T* norms,
 template <class St>
 void step_dispatch(const typename St::Store* fin, typename St::Store* fout, const uint8_t* solid,
                    typename St::Real* mac, int nx, int ny, int nz, typename St::Real uin,
-                   typename St::Real tau, typename St::Real smag, int serial) {
-    StepArgs<St> a{fin, fout, solid, mac, mac, nx, ny, nz, (int64_t)nx * ny * nz, uin, tau, smag};
+                   typename St::Real tau, typename St::Real smag, int serial, int fast) {
+    StepArgs<St> a{fin, fout, solid, mac, mac, nx, ny, nz, (int64_t)nx * ny * nz, uin, tau, smag, fast};
     if (serial) {
         step_serial_impl<St>(a);
     } else {
@@ -556,14 +679,16 @@ int oracle_init(int prec, void* f, void* mac, int64_t n, double uin) {
                 init_impl<StF64>((double*)f, (double*)mac, n, uin))
 }
 
+// collision: 0 = the reference's expressions in the reference's order, 1 = moment-space form
 int oracle_step(int prec, const void* fin, void* fout, const uint8_t* solid, void* mac, int nx, int ny, int nz,
-                double uin, double tau, double smag, int serial) {
+                double uin, double tau, double smag, int serial, int collision) {
     if (nx < 3 || ny < 3 || nz < 3) return -2;
+    if (collision != 0 && collision != 1) return -1;
     WT_DISPATCH(prec,
-                step_dispatch<StF32>((const float*)fin, (float*)fout, solid, (float*)mac, nx, ny, nz, (float)uin, (float)tau, (float)smag, serial),
-                step_dispatch<StF16>((const _Float16*)fin, (_Float16*)fout, solid, (float*)mac, nx, ny, nz, (float)uin, (float)tau, (float)smag, serial),
-                step_dispatch<StBF16>((const __bf16*)fin, (__bf16*)fout, solid, (float*)mac, nx, ny, nz, (float)uin, (float)tau, (float)smag, serial),
-                step_dispatch<StF64>((const double*)fin, (double*)fout, solid, (double*)mac, nx, ny, nz, uin, tau, smag, serial))
+                step_dispatch<StF32>((const float*)fin, (float*)fout, solid, (float*)mac, nx, ny, nz, (float)uin, (float)tau, (float)smag, serial, collision),
+                step_dispatch<StF16>((const _Float16*)fin, (_Float16*)fout, solid, (float*)mac, nx, ny, nz, (float)uin, (float)tau, (float)smag, serial, collision),
+                step_dispatch<StBF16>((const __bf16*)fin, (__bf16*)fout, solid, (float*)mac, nx, ny, nz, (float)uin, (float)tau, (float)smag, serial, collision),
+                step_dispatch<StF64>((const double*)fin, (double*)fout, solid, (double*)mac, nx, ny, nz, uin, tau, smag, serial, collision))
 }
 
 // out_ref is float* for prec 0-2 and double* for prec 3

@@ -41,7 +41,7 @@ def lib():
         vp, i32, i64, f32, f64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
         L.oracle_num_threads.argtypes = [i32]
         L.oracle_init.argtypes = [i32, vp, vp, i64, f64]
-        L.oracle_step.argtypes = [i32, vp, vp, vp, vp, i32, i32, i32, f64, f64, f64, i32]
+        L.oracle_step.argtypes = [i32, vp, vp, vp, vp, i32, i32, i32, f64, f64, f64, i32, i32]
         L.oracle_force.argtypes = [i32, vp, vp, i32, i32, i32, vp, vp, vp]
         L.oracle_mass.argtypes = [i32, vp, vp, i64, vp]
         L.oracle_advect_f32.argtypes = [vp, vp, vp, vp, i32, i32, i32, i64, f32, f32, f32, i32, f32, f32, f32, f32, f32]
@@ -80,7 +80,8 @@ def _chk(rc, what):
 class Lattice:
     """The reference Solver's device state held in host numpy arrays (server/lbm.py:398-413)."""
 
-    def __init__(self, dims, prec=F32):
+    def __init__(self, dims, prec=F32, collision=0):
+        self.collision = int(collision)  # 0 reference order, 1 moment-space form
         self.nx, self.ny, self.nz = (int(d) for d in dims)
         self.n = n = self.nx * self.ny * self.nz
         self.prec = prec
@@ -99,7 +100,7 @@ class Lattice:
         for _ in range(int(steps)):
             _chk(L.oracle_step(self.prec, _p(self.f[self.cur]), _p(self.f[1 - self.cur]), _p(self.solid),
                                _p(self.mac), self.nx, self.ny, self.nz, float(uin), float(tau), float(smag),
-                               1 if serial else 0), 'step')
+                               1 if serial else 0, self.collision), 'step')
             self.cur ^= 1
 
     def forces(self):

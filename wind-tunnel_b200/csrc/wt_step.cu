@@ -3,37 +3,58 @@
 // Semantics: step_kernel of RICKxxROLLING/wind-tunnel server/lbm.py:72-166.
 //
 // One step = two launches:
-//   k_step_bulk  -- every cell except the "current-read" faces below. Interior cells pull
-//                   and collide; x = 0 inlet cells; face cells whose interior neighbour has
-//                   a LARGER linear index read that neighbour's mac from the previous step
-//                   (mac_prev); outlet cells x = nx-1 with interior y, z take the current
-//                   value of their x = nx-2 neighbour from the adjacent lane by shuffle.
+//   k_step_bulk  -- every cell except the "current-read" faces below. Each thread owns V
+//                   consecutive cells of one x-row. Interior cells pull and collide; x = 0
+//                   inlet cells; face cells whose interior neighbour has a LARGER linear
+//                   index read that neighbour's mac from the previous step (mac_prev); the
+//                   outlet cell x = nx-1 of an interior row takes the current values of its
+//                   x = nx-2 neighbour, which the same thread has just computed.
 //   k_step_faces -- the z = nz-1 plane and the y = ny-1 rows of interior z (x > 0): their
 //                   neighbour has a SMALLER linear index, so they read the mac that
 //                   k_step_bulk just wrote (mac_cur).
-// This is exactly the value each face cell sees when the reference launch runs in tid
+// That is exactly the value each face cell sees when the reference launch runs in tid
 // order (Warp's CPU backend), and it is deterministic, unlike the single-launch race of
 // server/lbm.py:87 vs :166 on a GPU.
 //
+// Memory: population i of the pull source of cell idx is src[i][idx] with
+// src[i] = fin + i*n - (c_ix + c_iy*nx + c_iz*nx*ny), so every load is one base pointer
+// (kernel parameter, uniform) plus idx. A thread whose V cells are all plain interior fluid
+// (the common case) loads each population with one aligned V-wide vector load, plus one
+// scalar for the ±x-shifted ones, and stores each output population with one vector store.
+//
 // mac is double-buffered: the step that writes f[b] writes mac[b]. Every step writes mac
-// for the shell of interior cells that faces read (coordinates 1 or n-2); with
-// mac_all set (the last step before a frame) every cell writes it, as the reference does.
+// for the shell of interior cells that faces read (coordinates 1 or n-2); with mac_all set
+// (the last step before a frame) every cell writes it, as the reference does.
+//
+// Arithmetic keeps the reference's association order (the library is built without FMA
+// contraction). Two rewrites are exact: a leading "0.0 +" of a generated sum is dropped
+// (it can only turn -0.0 into +0.0, which no later operation can observe here), and the
+// term 0.5*cu*cu is shared by opposite directions (cu of the opposite direction is the
+// exact negation).
+#include <algorithm>
+
 #include "wt_common.cuh"
 
 namespace wt {
 
-template <class T>
+template <class S, class T>
 struct StepArgs {
-    const void* fin;
-    void* fout;
+    const S* src[Q];   // pull source bases, see above
+    S* dst[Q];         // fout + i*n
+    const S* fin;
     const T* mac_prev;
     T* mac_cur;
     const uint8_t* solid;
     const uint8_t* code;
     int32_t nx, ny, nz, n, nxy;
-    FastDiv dnx, dnxy;
-    T uin, tau, smag;
+    FastDiv dnx, dny, dny2;
+    T uin, tau, csmag;  // csmag = 25.4558441 * smag * smag, evaluated in T left to right
     int32_t mac_all;
+    // streaming kernel: 16-byte aligned copy bases (src[i] rounded down) and the remainders
+    const S* chunk_src[Q];
+    int32_t chunk_r[Q];
+    int32_t* status;           // device word for bounded-wait failures (may be null)
+    int32_t test_skip_chunk;   // test hook: when > 0, chunk test_skip_chunk-1 is never loaded
 };
 
 template <class T>
@@ -48,11 +69,11 @@ __device__ __forceinline__ void store_mac(T* mac, int32_t idx, T a, T b, T c, T 
 template <class T>
 __device__ __forceinline__ void load_mac(const T* mac, int32_t idx, T& a, T& b, T& c, T& d) {
     if constexpr (sizeof(T) == 4) {
-        float4 v = reinterpret_cast<const float4*>(mac)[idx];
+        const float4 v = reinterpret_cast<const float4*>(mac)[idx];
         a = v.x; b = v.y; c = v.z; d = v.w;
     } else {
-        double2 v0 = reinterpret_cast<const double2*>(mac)[2 * idx];
-        double2 v1 = reinterpret_cast<const double2*>(mac)[2 * idx + 1];
+        const double2 v0 = reinterpret_cast<const double2*>(mac)[2 * idx];
+        const double2 v1 = reinterpret_cast<const double2*>(mac)[2 * idx + 1];
         a = v0.x; b = v0.y; c = v1.x; d = v1.y;
     }
 }
@@ -60,10 +81,61 @@ __device__ __forceinline__ void load_mac(const T* mac, int32_t idx, T& a, T& b, 
 template <class T>
 __device__ __forceinline__ T clampv(T x, T lo, T hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
+// aligned vector of V stored values
+template <class S, int V>
+struct SVec {
+    S v[V];
+};
+template <class S, int V>
+__device__ __forceinline__ SVec<S, V> vload(const S* p) {
+    SVec<S, V> r;
+    constexpr int B = (int)sizeof(S) * V;
+    static_assert(B == 4 || B == 8 || B == 16 || B == 32, "vector width");
+    if constexpr (B == 4) {
+        const uint32_t u = *reinterpret_cast<const uint32_t*>(p);
+        memcpy(&r, &u, 4);
+    } else if constexpr (B == 8) {
+        const uint2 u = *reinterpret_cast<const uint2*>(p);
+        memcpy(&r, &u, 8);
+    } else if constexpr (B == 16) {
+        const uint4 u = *reinterpret_cast<const uint4*>(p);
+        memcpy(&r, &u, 16);
+    } else {
+        const uint4 u0 = reinterpret_cast<const uint4*>(p)[0];
+        const uint4 u1 = reinterpret_cast<const uint4*>(p)[1];
+        memcpy(&r, &u0, 16);
+        memcpy(reinterpret_cast<char*>(&r) + 16, &u1, 16);
+    }
+    return r;
+}
+template <class S, int V>
+__device__ __forceinline__ void vstore(S* p, const SVec<S, V>& r) {
+    constexpr int B = (int)sizeof(S) * V;
+    if constexpr (B == 4) {
+        uint32_t u;
+        memcpy(&u, &r, 4);
+        *reinterpret_cast<uint32_t*>(p) = u;
+    } else if constexpr (B == 8) {
+        uint2 u;
+        memcpy(&u, &r, 8);
+        *reinterpret_cast<uint2*>(p) = u;
+    } else if constexpr (B == 16) {
+        uint4 u;
+        memcpy(&u, &r, 16);
+        *reinterpret_cast<uint4*>(p) = u;
+    } else {
+        uint4 u0, u1;
+        memcpy(&u0, &r, 16);
+        memcpy(&u1, reinterpret_cast<const char*>(&r) + 16, 16);
+        reinterpret_cast<uint4*>(p)[0] = u0;
+        reinterpret_cast<uint4*>(p)[1] = u1;
+    }
+}
+
 // Equilibrium face populations from (br, bux, buy, buz) (server/lbm.py:104-107).
 template <class P>
-__device__ __forceinline__ void face_eq(typename P::S* fout, int64_t n, int32_t idx, typename P::T br,
-                                        typename P::T bux, typename P::T buy, typename P::T buz) {
+__device__ __forceinline__ void face_eq(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
+                                        typename P::T br, typename P::T bux, typename P::T buy, typename P::T buz) {
     using T = typename P::T;
     const T bsq = (T)1.5 * (bux * bux + buy * buy + buz * buz);
     unroll<0, Q>([&](auto ic) {
@@ -76,7 +148,7 @@ __device__ __forceinline__ void face_eq(typename P::S* fout, int64_t n, int32_t 
         if constexpr (cz(i) > 0) s = s + buz;
         if constexpr (cz(i) < 0) s = s - buz;
         const T bc = (T)3.0 * s;
-        st_pop<P, i>(fout + (int64_t)i * n + idx, (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq));
+        st_pop<P, i>(a.dst[i] + idx, (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq));
     });
 }
 
@@ -96,58 +168,31 @@ __device__ __forceinline__ void face_values(int32_t x, int32_t y, int32_t z, int
     }
 }
 
-// Interior cell: pull, bounce-back, moments, regularized Smagorinsky collision
-// (server/lbm.py:110-166). Returns the macroscopic values written to mac.
-template <class P>
-__device__ __forceinline__ void interior(const StepArgs<typename P::T>& a, int32_t idx, int32_t x, uint8_t code,
-                                         typename P::T& oux, typename P::T& ouy, typename P::T& ouz,
-                                         typename P::T& orho) {
-    using T = typename P::T;
-    using S = typename P::S;
-    const S* __restrict__ fin = static_cast<const S*>(a.fin);
-    S* __restrict__ fout = static_cast<S*>(a.fout);
-    const int64_t n = a.n;
-    const int32_t sy = a.nx, sz = a.nxy;
-    T f[Q];
-    f[0] = ld_pop<P, 0>(fin + idx);
-    if (!(code & CODE_NEAR)) {
-        unroll<1, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            const int32_t off = cx(i) + cy(i) * sy + cz(i) * sz;
-            f[i] = ld_pop<P, i>(fin + (int64_t)i * n + (idx - off));
-        });
-    } else {
-        unroll<1, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            const int32_t off = cx(i) + cy(i) * sy + cz(i) * sz;
-            const int t = a.solid[idx - off];
-            if (t == 0) {
-                f[i] = ld_pop<P, i>(fin + (int64_t)i * n + (idx - off));
-            } else {
-                f[i] = ld_pop<P, opp(i)>(fin + (int64_t)opp(i) * n + idx);
-                if constexpr (cx(i) != 0) {
-                    if (t == 2) f[i] = f[i] + (T)(6.0 * wd(i) * cx(i)) * a.uin;
-                }
-            }
-        });
-    }
-    T rho = (T)0.0, jx = (T)0.0, jy = (T)0.0, jz = (T)0.0;
-    unroll<0, Q>([&](auto ic) { constexpr int i = decltype(ic)::value; rho = rho + f[i]; });
+// sum of c-signed terms in the generator's order with the leading "0.0 +" dropped
+template <int AX, class T>
+__device__ __forceinline__ T csum(const T (&f)[Q]) {
+    T acc = (T)0.0;
+    bool first = true;
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        if constexpr (cx(i) > 0) jx = jx + f[i];
-        if constexpr (cx(i) < 0) jx = jx - f[i];
+        constexpr int c = AX == 0 ? cx(i) : (AX == 1 ? cy(i) : cz(i));
+        if constexpr (c != 0) {
+            if (first) acc = c > 0 ? f[i] : -f[i];
+            else acc = c > 0 ? acc + f[i] : acc - f[i];
+            first = false;
+        }
     });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cy(i) > 0) jy = jy + f[i];
-        if constexpr (cy(i) < 0) jy = jy - f[i];
-    });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cz(i) > 0) jz = jz + f[i];
-        if constexpr (cz(i) < 0) jz = jz - f[i];
-    });
+    return acc;
+}
+
+// Regularized Smagorinsky collision of one cell (server/lbm.py:125-166). f holds the
+// pulled populations on entry and the post-collision populations on exit.
+template <class T>
+__device__ __forceinline__ void collide(T (&f)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy, T& ouz,
+                                        T& orho) {
+    T rho = f[0];
+    unroll<1, Q>([&](auto ic) { rho = rho + f[decltype(ic)::value]; });
+    const T jx = csum<0>(f), jy = csum<1>(f), jz = csum<2>(f);
     const T ir = (T)1.0 / rho;
     T ux = jx * ir, uy = jy * ir, uz = jz * ir;
     const T um = sqrt(ux * ux + uy * uy + uz * uz);
@@ -156,54 +201,64 @@ __device__ __forceinline__ void interior(const StepArgs<typename P::T>& a, int32
         ux = ux * sc; uy = uy * sc; uz = uz * sc;
     }
     const T usq = (T)1.5 * (ux * ux + uy * uy + uz * uz);
-    // f[] now holds the non-equilibrium parts d_i = f_i - e_i; e[] the equilibria
     T e[Q];
+    // e_i = w rho (1 + cu + 0.5 cu cu - usq), d_i = f_i - e_i (f[] becomes d[])
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        T s = (T)0.0;
-        if constexpr (cx(i) > 0) s = s + ux;
-        if constexpr (cx(i) < 0) s = s - ux;
-        if constexpr (cy(i) > 0) s = s + uy;
-        if constexpr (cy(i) < 0) s = s - uy;
-        if constexpr (cz(i) > 0) s = s + uz;
-        if constexpr (cz(i) < 0) s = s - uz;
-        const T cu = (T)3.0 * s;
-        e[i] = (T)wd(i) * rho * ((T)1.0 + cu + (T)0.5 * cu * cu - usq);
-        f[i] = f[i] - e[i];
+        if constexpr (i == 0) {
+            e[0] = (T)wd(0) * rho * ((T)1.0 - usq);
+            f[0] = f[0] - e[0];
+        } else if constexpr (opp(i) > i) {  // handle the pair (i, opp(i)) together
+            constexpr int o = opp(i);
+            T s;
+            bool first = true;
+            if constexpr (cx(i) != 0) { s = cx(i) > 0 ? ux : -ux; first = false; }
+            if constexpr (cy(i) != 0) {
+                if (first) s = cy(i) > 0 ? uy : -uy;
+                else s = cy(i) > 0 ? s + uy : s - uy;
+                first = false;
+            }
+            if constexpr (cz(i) != 0) {
+                if (first) s = cz(i) > 0 ? uz : -uz;
+                else s = cz(i) > 0 ? s + uz : s - uz;
+            }
+            const T cu = (T)3.0 * s;
+            const T q = (T)0.5 * cu * cu;
+            const T wr = (T)wd(i) * rho;
+            e[i] = wr * ((T)1.0 + cu + q - usq);
+            e[o] = wr * ((T)1.0 - cu + q - usq);
+            f[i] = f[i] - e[i];
+            f[o] = f[o] - e[o];
+        }
     });
-    T pxx = (T)0.0, pyy = (T)0.0, pzz = (T)0.0, pxy = (T)0.0, pxz = (T)0.0, pyz = (T)0.0;
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cx(i) != 0) pxx = pxx + f[i];
-    });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cy(i) != 0) pyy = pyy + f[i];
-    });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cz(i) != 0) pzz = pzz + f[i];
-    });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cx(i) * cy(i) > 0) pxy = pxy + f[i];
-        if constexpr (cx(i) * cy(i) < 0) pxy = pxy - f[i];
-    });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cx(i) * cz(i) > 0) pxz = pxz + f[i];
-        if constexpr (cx(i) * cz(i) < 0) pxz = pxz - f[i];
-    });
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (cy(i) * cz(i) > 0) pyz = pyz + f[i];
-        if constexpr (cy(i) * cz(i) < 0) pyz = pyz - f[i];
-    });
+    T pxx, pyy, pzz, pxy, pxz, pyz;
+    {
+        bool fx = true, fy = true, fz = true, fxy = true, fxz = true, fyz = true;
+        pxx = pyy = pzz = pxy = pxz = pyz = (T)0.0;
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            if constexpr (cx(i) != 0) { pxx = fx ? f[i] : pxx + f[i]; fx = false; }
+            if constexpr (cy(i) != 0) { pyy = fy ? f[i] : pyy + f[i]; fy = false; }
+            if constexpr (cz(i) != 0) { pzz = fz ? f[i] : pzz + f[i]; fz = false; }
+            if constexpr (cx(i) * cy(i) != 0) {
+                pxy = fxy ? (cx(i) * cy(i) > 0 ? f[i] : -f[i]) : (cx(i) * cy(i) > 0 ? pxy + f[i] : pxy - f[i]);
+                fxy = false;
+            }
+            if constexpr (cx(i) * cz(i) != 0) {
+                pxz = fxz ? (cx(i) * cz(i) > 0 ? f[i] : -f[i]) : (cx(i) * cz(i) > 0 ? pxz + f[i] : pxz - f[i]);
+                fxz = false;
+            }
+            if constexpr (cy(i) * cz(i) != 0) {
+                pyz = fyz ? (cy(i) * cz(i) > 0 ? f[i] : -f[i]) : (cy(i) * cz(i) > 0 ? pyz + f[i] : pyz - f[i]);
+                fyz = false;
+            }
+        });
+    }
     const T qn = sqrt(pxx * pxx + pyy * pyy + pzz * pzz + (T)2.0 * (pxy * pxy + pxz * pxz + pyz * pyz));
-    T tau0 = a.tau;
-    const T sp = (T)x - (T)a.nx + (T)24.0;
+    T tau0 = tau;
+    const T sp = (T)x - (T)nx + (T)24.0;
     if (sp > (T)0.0) tau0 = tau0 + sp * (T)0.015;
-    const T tau_e = (T)0.5 * (tau0 + sqrt(tau0 * tau0 + (T)25.4558441 * a.smag * a.smag * qn * ir));
+    const T tau_e = (T)0.5 * (tau0 + sqrt(tau0 * tau0 + csmag * qn * ir));
     const T keep = (T)1.0 - (T)1.0 / tau_e;
     const T tr3 = (pxx + pyy + pzz) * ((T)1.0 / (T)3.0);
     unroll<0, Q>([&](auto ic) {
@@ -211,103 +266,321 @@ __device__ __forceinline__ void interior(const StepArgs<typename P::T>& a, int32
         // the generator's ' + '.join(terms) + ' - tr3' (server/lbm.py:157-164)
         T qp;
         if constexpr (i == 0) {
-            qp = (T)0.0 - tr3;
+            qp = -tr3;
         } else {
             constexpr bool hx = cx(i) != 0, hy = cy(i) != 0, hz = cz(i) != 0;
-            T acc = hx ? pxx : (hy ? pyy : pzz);  // first present term
+            T acc = hx ? pxx : (hy ? pyy : pzz);
             if constexpr (hx && hy) acc = acc + pyy;
             if constexpr ((hx || hy) && hz) acc = acc + pzz;
-            if constexpr (cx(i) != 0 && cy(i) != 0) acc = acc + (T)(2 * cx(i) * cy(i)) * pxy;
-            if constexpr (cx(i) != 0 && cz(i) != 0) acc = acc + (T)(2 * cx(i) * cz(i)) * pxz;
-            if constexpr (cy(i) != 0 && cz(i) != 0) acc = acc + (T)(2 * cy(i) * cz(i)) * pyz;
+            if constexpr (hx && hy) acc = acc + (T)(2 * cx(i) * cy(i)) * pxy;
+            if constexpr (hx && hz) acc = acc + (T)(2 * cx(i) * cz(i)) * pxz;
+            if constexpr (hy && hz) acc = acc + (T)(2 * cy(i) * cz(i)) * pyz;
             qp = acc - tr3;
         }
-        st_pop<P, i>(fout + (int64_t)i * n + idx, e[i] + (T)(4.5 * wd(i)) * keep * qp);
+        f[i] = e[i] + (T)(4.5 * wd(i)) * keep * qp;
     });
     oux = ux; ouy = uy; ouz = uz; orho = rho;
 }
 
-enum Kind { K_NONE = 0, K_SOLID, K_INLET, K_FACE, K_OUTLET, K_INTERIOR, K_LATER };
+// fused multiply-add, rounded once (explicit: the library is built without contraction)
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
 
-template <int PREC>
-__global__ void __launch_bounds__(256) k_step_bulk(const StepArgs<typename Prec<PREC>::T> a) {
-    using P = Prec<PREC>;
-    using T = typename P::T;
-    using S = typename P::S;
-    const int32_t idx = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    const bool valid = idx < a.n;
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t z = valid ? (int32_t)a.dnxy.div((uint32_t)idx) : 0;
-    const int32_t r = idx - z * a.nxy;
-    const int32_t y = (int32_t)a.dnx.div((uint32_t)r);
-    const int32_t x = r - y * nx;
-    T mx = (T)0.0, my = (T)0.0, mz = (T)0.0, mr = (T)1.0;
-    int kind = K_NONE;
-    if (valid) {
-        const uint8_t code = a.code[idx];
-        const bool face = x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
-        if (code & CODE_SOLID) {
-            kind = K_SOLID;
-        } else if (x == 0) {
-            kind = K_INLET;
-            mx = a.uin;
-            face_eq<P>(static_cast<S*>(a.fout), a.n, idx, (T)1.0, a.uin, (T)0.0, (T)0.0);
-        } else if (face) {
-            if (z == nz - 1 || (y == ny - 1 && z > 0)) {
-                kind = K_LATER;
-            } else if (x == nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {
-                kind = K_OUTLET;
-            } else {
-                kind = K_FACE;
-                const int32_t cxi = min(max(x, 1), nx - 2), cyi = min(max(y, 1), ny - 2), czi = min(max(z, 1), nz - 2);
-                T px, py, pz, pr;
-                load_mac(a.mac_prev, cxi + nx * (cyi + ny * czi), px, py, pz, pr);
-                face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, mr, mx, my, mz);
-                face_eq<P>(static_cast<S*>(a.fout), a.n, idx, mr, mx, my, mz);
-            }
-        } else {
-            kind = K_INTERIOR;
-            interior<P>(a, idx, x, code, mx, my, mz, mr);
-        }
+// Moment-space form of the same regularized Smagorinsky collision (mathematically equal
+// to collide(): on D3Q19 the second moment of the second-order equilibrium is
+// rho (u u + I/3), so Pi_neq = sum_i f_i c_i c_i - rho (u u + I/3), and every output is
+// w_i (B + 3 rho c.u + 4.5 rho (c.u)^2 + c c : A) with A = 4.5 (1 - 1/tau_e) Pi_neq and
+// B = rho (1 - 1.5 u.u) - tr(A)/3). Opposite directions share all but the sign of the odd
+// term. About 200 floating-point operations per cell against 330 in the reference order.
+// With SHIFT the inputs and outputs are deviations v_i = f_i - w_i (the fp16/bf16 storage
+// form): the constant parts cancel analytically, which keeps small numbers small.
+// Every operation is an IEEE add/mul/fma/div/sqrt, so the oracle reproduces it exactly.
+template <class T, bool SHIFT>
+__device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy,
+                                             T& ouz, T& orho) {
+    const T s1 = v[1] + v[2], a1 = v[1] - v[2];
+    const T s3 = v[3] + v[4], a3 = v[3] - v[4];
+    const T s5 = v[5] + v[6], a5 = v[5] - v[6];
+    const T s7 = v[7] + v[8], a7 = v[7] - v[8];
+    const T s9 = v[9] + v[10], a9 = v[9] - v[10];
+    const T s11 = v[11] + v[12], a11 = v[11] - v[12];
+    const T s13 = v[13] + v[14], a13 = v[13] - v[14];
+    const T s15 = v[15] + v[16], a15 = v[15] - v[16];
+    const T s17 = v[17] + v[18], a17 = v[17] - v[18];
+    const T d7 = s7 + s9, d11 = s11 + s13, d15 = s15 + s17;
+    const T xxx = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
+    const T xxy = s7 - s9, xxz = s11 - s13, xyz = s15 - s17;
+    const T S = ((v[0] + s1) + (s3 + s5)) + ((d7 + d11) + d15);
+    const T jx = ((a1 + a7) + (a9 + a11)) + a13;
+    const T jy = ((a3 + a7) - (a9 - a15)) + a17;
+    const T jz = ((a5 + a11) - (a13 - a15)) - a17;
+    const T rho = SHIFT ? S + (T)1.0 : S;
+    const T ir = (T)1.0 / rho;
+    T ux = jx * ir, uy = jy * ir, uz = jz * ir;
+    T usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
+    if (usq > (T)0.1225) {  // |u| > 0.35 (server/lbm.py:131-135)
+        const T sc = (T)0.35 / sqrt(usq);
+        ux = ux * sc; uy = uy * sc; uz = uz * sc;
+        usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
     }
-    // outlet x = nx-1 (interior y, z): its neighbour x = nx-2 is the previous lane. nx is
-    // even, so idx of x = nx-1 is odd and never lane 0.
-    const T qx = __shfl_up_sync(0xffffffffu, mx, 1);
-    const T qy = __shfl_up_sync(0xffffffffu, my, 1);
-    const T qz = __shfl_up_sync(0xffffffffu, mz, 1);
-    const T qr = __shfl_up_sync(0xffffffffu, mr, 1);
-    if (kind == K_OUTLET) {
-        face_values<T>(x, y, z, nx, ny, nz, a.uin, qx, qy, qz, qr, mr, mx, my, mz);
-        face_eq<P>(static_cast<S*>(a.fout), a.n, idx, mr, mx, my, mz);
+    const T rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    const T t3 = (SHIFT ? S : rho) * ((T)1.0 / (T)3.0);
+    const T nxx = fmaT(-rux, ux, xxx - t3), nyy = fmaT(-ruy, uy, xyy - t3), nzz = fmaT(-ruz, uz, xzz - t3);
+    const T nxy = fmaT(-rux, uy, xxy), nxz = fmaT(-rux, uz, xxz), nyz = fmaT(-ruy, uz, xyz);
+    const T q1 = fmaT(nzz, nzz, fmaT(nyy, nyy, nxx * nxx));
+    const T q2 = fmaT(nyz, nyz, fmaT(nxz, nxz, nxy * nxy));
+    const T qn = sqrt(fmaT((T)2.0, q2, q1));
+    T tau0 = tau;
+    const T sp = (T)x - (T)(nx - 24);  // outlet sponge (server/lbm.py:149-151)
+    if (sp > (T)0.0) tau0 = fmaT(sp, (T)0.015, tau);
+    const T tau_e = (T)0.5 * (tau0 + sqrt(fmaT(tau0, tau0, csmag * qn * ir)));
+    const T keep = (T)1.0 - (T)1.0 / tau_e;
+    const T k45 = (T)4.5 * keep, k9 = (T)9.0 * keep;
+    const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
+    const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;  // 2 A_ab
+    const T tra3 = ((axx + ayy) + azz) * ((T)1.0 / (T)3.0);
+    const T B = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+    const T w0 = (T)wd(0), w1 = (T)wd(1), w2 = (T)wd(7);
+    const T w1x3 = (T)(3.0 * wd(1)), w2x3 = (T)(3.0 * wd(7));
+    v[0] = w0 * B;
+    const T bxx = B + axx, byy = B + ayy;
+    {
+        const T D = fmaT((T)4.5 * rux, ux, bxx), E = w1x3 * rux;
+        v[1] = fmaT(w1, D, E); v[2] = fmaT(w1, D, -E);
     }
-    if (kind == K_SOLID) { mx = (T)0.0; my = (T)0.0; mz = (T)0.0; mr = (T)1.0; }
-    if (kind != K_NONE && kind != K_LATER) {
-        const bool shell = !(x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) &&
-                           (x == 1 || x == nx - 2 || y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-        if (a.mac_all || shell) store_mac(a.mac_cur, idx, mx, my, mz, mr);
+    {
+        const T D = fmaT((T)4.5 * ruy, uy, byy), E = w1x3 * ruy;
+        v[3] = fmaT(w1, D, E); v[4] = fmaT(w1, D, -E);
     }
+    {
+        const T D = fmaT((T)4.5 * ruz, uz, B + azz), E = w1x3 * ruz;
+        v[5] = fmaT(w1, D, E); v[6] = fmaT(w1, D, -E);
+    }
+    const T pxy = bxx + ayy, pxz = bxx + azz, pyz = byy + azz;
+    {
+        const T su = ux + uy, rs = rux + ruy;
+        const T D = fmaT((T)4.5 * rs, su, pxy + axy), E = w2x3 * rs;
+        v[7] = fmaT(w2, D, E); v[8] = fmaT(w2, D, -E);
+    }
+    {
+        const T su = ux - uy, rs = rux - ruy;
+        const T D = fmaT((T)4.5 * rs, su, pxy - axy), E = w2x3 * rs;
+        v[9] = fmaT(w2, D, E); v[10] = fmaT(w2, D, -E);
+    }
+    {
+        const T su = ux + uz, rs = rux + ruz;
+        const T D = fmaT((T)4.5 * rs, su, pxz + axz), E = w2x3 * rs;
+        v[11] = fmaT(w2, D, E); v[12] = fmaT(w2, D, -E);
+    }
+    {
+        const T su = ux - uz, rs = rux - ruz;
+        const T D = fmaT((T)4.5 * rs, su, pxz - axz), E = w2x3 * rs;
+        v[13] = fmaT(w2, D, E); v[14] = fmaT(w2, D, -E);
+    }
+    {
+        const T su = uy + uz, rs = ruy + ruz;
+        const T D = fmaT((T)4.5 * rs, su, pyz + ayz), E = w2x3 * rs;
+        v[15] = fmaT(w2, D, E); v[16] = fmaT(w2, D, -E);
+    }
+    {
+        const T su = uy - uz, rs = ruy - ruz;
+        const T D = fmaT((T)4.5 * rs, su, pyz - ayz), E = w2x3 * rs;
+        v[17] = fmaT(w2, D, E); v[18] = fmaT(w2, D, -E);
+    }
+    oux = ux; ouy = uy; ouz = uz; orho = rho;
 }
 
-template <int PREC>
-__global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec<PREC>::T> a) {
+// collision dispatch: FAST selects the moment-space form, on deviations for shifted storage
+template <class P, bool FAST>
+__device__ __forceinline__ void collide_any(typename P::T (&f)[Q], int32_t x, int32_t nx, typename P::T tau,
+                                            typename P::T csmag, typename P::T& ux, typename P::T& uy,
+                                            typename P::T& uz, typename P::T& rho) {
+    if constexpr (FAST) collide_fast<typename P::T, P::shifted>(f, x, nx, tau, csmag, ux, uy, uz, rho);
+    else collide<typename P::T>(f, x, nx, tau, csmag, ux, uy, uz, rho);
+}
+
+// population value as the collision of mode FAST takes it: f_i (+ w_i undone for shifted
+// storage in the exact form), or the stored deviation itself in the fast form
+template <class P, bool FAST, int I>
+__device__ __forceinline__ typename P::T ld_in(const typename P::S* p) {
+    if constexpr (FAST) return P::to(*p);
+    else return ld_pop<P, I>(p);
+}
+template <class P, bool FAST, int I>
+__device__ __forceinline__ void st_out(typename P::S* p, typename P::T v) {
+    if constexpr (FAST) *p = P::from(v);
+    else st_pop<P, I>(p, v);
+}
+
+// Pull of one cell with bounce-back and moving belt where a source is non-fluid
+// (server/lbm.py:110-124).
+template <class P, bool FAST>
+__device__ __forceinline__ void pull_generic(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
+                                             bool near, typename P::T (&f)[Q]) {
+    using T = typename P::T;
+    f[0] = ld_in<P, FAST, 0>(a.src[0] + idx);
+    unroll<1, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if (!near) {
+            f[i] = ld_in<P, FAST, i>(a.src[i] + idx);
+        } else {
+            const int32_t off = cx(i) + cy(i) * a.nx + cz(i) * a.nxy;
+            const int t = a.solid[idx - off];
+            if (t == 0) {
+                f[i] = ld_in<P, FAST, i>(a.src[i] + idx);
+            } else {
+                // bounce-back; in deviation form w_opp(i) = w_i, so the value carries over
+                f[i] = ld_in<P, FAST, opp(i)>(a.fin + (int64_t)opp(i) * a.n + idx);
+                if constexpr (cx(i) != 0) {
+                    if (t == 2) f[i] = f[i] + (T)(6.0 * wd(i) * cx(i)) * a.uin;
+                }
+            }
+        }
+    });
+}
+
+template <class P, bool FAST>
+__device__ __forceinline__ void store_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
+                                           const typename P::T (&f)[Q]) {
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        st_out<P, FAST, i>(a.dst[i] + idx, f[i]);
+    });
+}
+
+// One cell outside the vector fast path: inlet, "previous-read" faces, solids and fluid
+// cells next to non-fluid cells. Cells that k_step_faces owns are skipped.
+template <class P, bool FAST>
+__device__ __forceinline__ void general_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx, int32_t x,
+                                             int32_t y, int32_t z, uint32_t code, bool face_row, bool row_shell) {
+    using T = typename P::T;
+    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
+    const bool later = x > 0 && (face_row ? (z == nz - 1 || (y == ny - 1 && z > 0)) : x == nx - 1);
+    if (later) return;
+    bool write = a.mac_all;
+    T ox, oy, oz, orr;
+    if (code & CODE_SOLID) {
+        ox = (T)0.0; oy = (T)0.0; oz = (T)0.0; orr = (T)1.0;
+        write = write || (row_shell || (!face_row && (x == 1 || x == nx - 2)));
+    } else if (x == 0) {
+        ox = a.uin; oy = (T)0.0; oz = (T)0.0; orr = (T)1.0;
+        face_eq<P>(a, idx, (T)1.0, a.uin, (T)0.0, (T)0.0);
+    } else if (face_row) {
+        const int32_t cxi = min(max(x, 1), nx - 2), cyi = min(max(y, 1), ny - 2), czi = min(max(z, 1), nz - 2);
+        T px, py, pz, pr;
+        load_mac(a.mac_prev, cxi + nx * (cyi + ny * czi), px, py, pz, pr);
+        face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, orr, ox, oy, oz);
+        face_eq<P>(a, idx, orr, ox, oy, oz);
+    } else {
+        T f[Q];
+        pull_generic<P, FAST>(a, idx, (code & CODE_NEAR) != 0, f);
+        collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, ox, oy, oz, orr);
+        store_cell<P, FAST>(a, idx, f);
+        write = write || row_shell || x == 1 || x == nx - 2;
+    }
+    if (write) store_mac(a.mac_cur, idx, ox, oy, oz, orr);
+}
+
+template <int PREC, bool FAST, int V, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_bulk(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
     using P = Prec<PREC>;
     using T = typename P::T;
     using S = typename P::S;
     const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int32_t idx0 = t * V;
+    if (idx0 >= a.n) return;
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t nplane = a.nxy;
-    if (t >= nplane + nx * (nz - 2)) return;
+    const int32_t row = (int32_t)a.dnx.div((uint32_t)idx0);
+    const int32_t x0 = idx0 - row * nx;
+    const int32_t z = (int32_t)a.dny.div((uint32_t)row);
+    const int32_t y = row - z * ny;
+    const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+    const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
+
+    uint32_t codes;
+    if constexpr (V == 4) codes = *reinterpret_cast<const uint32_t*>(a.code + idx0);
+    else if constexpr (V == 2) codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
+    else codes = a.code[idx0];
+
+    if (!face_row && x0 > 0 && x0 + V <= nx - 1 && codes == 0) {
+        // ---- fast path: V plain interior fluid cells, vector loads and stores ----
+        T f[V][Q];
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            const S* p = a.src[i] + idx0;
+            if constexpr (V == 1) {
+                f[0][i] = ld_in<P, FAST, i>(p);
+            } else {
+                const SVec<S, V> v = vload<S, V>(p + cx(i));  // aligned: the shift cancels
+                if constexpr (cx(i) == 0) {
+#pragma unroll
+                    for (int k = 0; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k]);
+                } else if constexpr (cx(i) > 0) {
+                    f[0][i] = ld_in<P, FAST, i>(p);
+#pragma unroll
+                    for (int k = 1; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k - 1]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < V - 1; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k + 1]);
+                    f[V - 1][i] = ld_in<P, FAST, i>(p + V - 1);
+                }
+            }
+        });
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            T ux, uy, uz, rho;
+            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, ux, uy, uz, rho);
+            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2)
+                store_mac(a.mac_cur, idx0 + k, ux, uy, uz, rho);
+        }
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            if constexpr (V == 1) {
+                st_out<P, FAST, i>(a.dst[i] + idx0, f[0][i]);
+            } else {
+                SVec<S, V> v;
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    if constexpr (P::shifted && !FAST) v.v[k] = P::from(f[k][i] - (T)wd(i));
+                    else v.v[k] = P::from(f[k][i]);
+                }
+                vstore<S, V>(a.dst[i] + idx0, v);
+            }
+        });
+        return;
+    }
+
+    // ---- general path: cell by cell (faces, inlet, solids, cells next to solids) ----
+#pragma unroll 1
+    for (int k = 0; k < V; ++k)
+        general_cell<P, FAST>(a, idx0 + k, x0 + k, y, z, (codes >> (8 * k)) & 0xffu, face_row, row_shell);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
+    const int32_t nplane = a.nxy, nrows = nx * (nz - 2);
+    if (t >= nplane + nrows + (ny - 2) * (nz - 2)) return;
     int32_t x, y, z;
-    if (t < nplane) {
+    if (t < nplane) {  // z = nz-1 plane
         z = nz - 1;
         y = (int32_t)a.dnx.div((uint32_t)t);
         x = t - y * nx;
-    } else {
+    } else if (t < nplane + nrows) {  // y = ny-1 rows of interior z
         const int32_t t2 = t - nplane;
-        const int32_t row = (int32_t)a.dnx.div((uint32_t)t2);
-        z = 1 + row;
+        const int32_t r = (int32_t)a.dnx.div((uint32_t)t2);
+        z = 1 + r;
         y = ny - 1;
-        x = t2 - row * nx;
+        x = t2 - r * nx;
+    } else {  // outlet x = nx-1 of interior rows: its x = nx-2 neighbour was just updated
+        const int32_t t3 = t - nplane - nrows;
+        const int32_t r = (int32_t)a.dny2.div((uint32_t)t3);
+        z = 1 + r;
+        y = 1 + (t3 - r * (ny - 2));
+        x = nx - 1;
     }
     if (x == 0) return;
     const int32_t idx = x + nx * (y + ny * z);
@@ -319,33 +592,308 @@ __global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec
     T px, py, pz, pr, br, bux, buy, buz;
     load_mac(a.mac_cur, cxi + nx * (cyi + ny * czi), px, py, pz, pr);
     face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, br, bux, buy, buz);
-    face_eq<P>(static_cast<S*>(a.fout), a.n, idx, br, bux, buy, buz);
+    face_eq<P>(a, idx, br, bux, buy, buz);
     if (a.mac_all) store_mac(a.mac_cur, idx, bux, buy, buz, br);
+}
+
+// ---------------------------------------------------------------------------------
+// Streaming form of the bulk kernel: shared-memory staging through bulk async copies.
+//
+// With pull streaming, the destination cells [c0, c0 + L) read population i from the
+// contiguous source range src[i][c0 .. c0 + L): every population of a chunk of cells is
+// one 1-D bulk copy (cp.async.bulk, no tensor map, no multicast). The copy starts at the
+// 16-byte boundary at or below the range (chunk_src[i] = src[i] - chunk_r[i]) and is one
+// vector longer, so the cell at chunk offset c is stage[i][chunk_r[i] + c]. One elected
+// thread issues the 19 population copies plus the chunk's code bytes into a stage and
+// arms its mbarrier with the byte count; all threads wait on the barrier (bounded), update
+// the chunk from shared memory and store to global memory, then the stage is refilled
+// with the chunk S positions ahead. Persistent CTAs walk chunks blockIdx.x + j*gridDim.x.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after about a second (each try_wait may itself suspend briefly).
+constexpr uint32_t WAIT_LIMIT = 1u << 20;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 32) __nanosleep(256);
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <class S, int L>
+struct StreamLayout {
+    static constexpr int VEC = 16 / (int)sizeof(S);
+    static constexpr int LP = L + VEC;                        // elements per population buffer
+    static constexpr int POP_BYTES = LP * (int)sizeof(S);     // multiple of 16
+    static constexpr int STAGE_BYTES = Q * POP_BYTES + L;     // populations + code bytes
+    static_assert(L % 16 == 0, "chunk length");
+};
+
+template <int PREC, int L, int NS>
+__device__ __forceinline__ void stream_issue(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                             unsigned char* smem, uint64_t* bar, int32_t chunk, int st) {
+    using S = typename Prec<PREC>::S;
+    using LY = StreamLayout<S, L>;
+    if (chunk + 1 == a.test_skip_chunk) return;  // test hook: leave the stage empty
+    const int32_t c0 = chunk * L;
+    const int32_t len = min(L, a.n - c0);
+    const int32_t len16 = (len + LY::VEC - 1) / LY::VEC * LY::VEC;
+    const uint32_t pop_bytes = (uint32_t)((len16 + LY::VEC) * (int)sizeof(S));
+    const uint32_t code_bytes = (uint32_t)((len + 15) / 16 * 16);
+    unsigned char* stage = smem + (size_t)st * LY::STAGE_BYTES;
+    mbar_arrive_expect_tx(&bar[st], Q * pop_bytes + code_bytes);
+#pragma unroll 1
+    for (int i = 0; i < Q; ++i) bulk_g2s(stage + i * LY::POP_BYTES, a.chunk_src[i] + c0, pop_bytes, &bar[st]);
+    bulk_g2s(stage + Q * LY::POP_BYTES, a.code + c0, code_bytes, &bar[st]);
+}
+
+template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    using S = typename P::S;
+    using LY = StreamLayout<S, L>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NS * LY::STAGE_BYTES);
+    const int32_t nchunks = (a.n + L - 1) / L;
+    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < NS; ++st) mbar_init(&bar[st], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t inflight = 0;  // thread 0: stages with a copy issued and not yet consumed
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < NS; ++st) {
+            const int32_t k = blockIdx.x + st * gridDim.x;
+            if (k < nchunks) {
+                stream_issue<PREC, L, NS>(a, smem, bar, k, st);
+                inflight |= 1u << st;
+            }
+        }
+    }
+#pragma unroll 1
+    for (int32_t j = 0;; ++j) {
+        const int32_t k = blockIdx.x + j * gridDim.x;
+        if (k >= nchunks) break;
+        const int st = j % NS;
+        const uint32_t parity = (uint32_t)((j / NS) & 1);
+        const bool ok = mbar_wait(&bar[st], parity);
+        if (__syncthreads_or(!ok)) {  // one decision for the whole CTA
+            // the stage never filled: report, drain the copies this CTA still has in flight
+            // (bounded), and leave; the tunnel's state is invalid until the next reset
+            if (a.status && threadIdx.x == 0) atomicExch(a.status, WT_ERR_TIMEOUT);
+            if (threadIdx.x == 0) {
+                for (int d = 1; d < NS; ++d) {
+                    const int s2 = (st + d) % NS;
+                    const int32_t j2 = j + d;
+                    if ((inflight >> s2) & 1u) mbar_wait(&bar[s2], (uint32_t)((j2 / NS) & 1));
+                }
+            }
+            return;
+        }
+        const unsigned char* stage = smem + (size_t)st * LY::STAGE_BYTES;
+        const uint8_t* codes = stage + Q * LY::POP_BYTES;
+        const int32_t c0 = k * L;
+        const int32_t len = min(L, a.n - c0);
+#pragma unroll 1
+        for (int32_t c = threadIdx.x; c < len; c += THREADS) {
+            const int32_t idx = c0 + c;
+            const int32_t row = (int32_t)a.dnx.div((uint32_t)idx);
+            const int32_t x = idx - row * nx;
+            const int32_t z = (int32_t)a.dny.div((uint32_t)row);
+            const int32_t y = row - z * ny;
+            const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+            const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
+            const uint32_t code = codes[c];
+            if (!face_row && x > 0 && x < nx - 1 && code == 0) {
+                T f[Q];
+                unroll<0, Q>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    const S* sp = reinterpret_cast<const S*>(stage + i * LY::POP_BYTES) + a.chunk_r[i] + c;
+                    f[i] = ld_in<P, FAST, i>(sp);
+                });
+                T ux, uy, uz, rho;
+                collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, ux, uy, uz, rho);
+                store_cell<P, FAST>(a, idx, f);
+                if (a.mac_all || row_shell || x == 1 || x == nx - 2) store_mac(a.mac_cur, idx, ux, uy, uz, rho);
+            } else {
+                general_cell<P, FAST>(a, idx, x, y, z, code, face_row, row_shell);
+            }
+        }
+        __syncthreads();  // every thread is done with this stage
+        if (threadIdx.x == 0) {
+            inflight &= ~(1u << st);
+            const int32_t kn = k + NS * gridDim.x;
+            if (kn < nchunks) {
+                fence_proxy_async_smem();
+                stream_issue<PREC, L, NS>(a, smem, bar, kn, st);
+                inflight |= 1u << st;
+            }
+        }
+    }
+}
+
+// Tile variants of the step kernel. Direct-load forms (kind 0): cells per thread (V),
+// threads per block, minimum resident blocks per SM (bounds registers). Streaming forms
+// (kind 1): chunk length L, pipeline stages NS, threads per block, blocks per SM.
+// wt_grid.tile selects one (0 = the default for the precision); autotune.py times them.
+struct StepVariant {
+    int id, kind, v, block, minb, chunk, stages;
+    int (*launch)(const void* args, int32_t n, cudaStream_t st);
+};
+
+static int num_sms() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+template <int PREC, bool FAST, int V, int BLOCK, int MINB>
+static int launch_bulk(const void* args, int32_t n, cudaStream_t st) {
+    using P = Prec<PREC>;
+    const auto& a = *static_cast<const StepArgs<typename P::S, typename P::T>*>(args);
+    const int32_t nthreads = n / V;
+    k_step_bulk<PREC, FAST, V, BLOCK, MINB><<<(unsigned)((nthreads + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
+    return WT_OK;
+}
+
+template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB>
+static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
+    using P = Prec<PREC>;
+    using LY = StreamLayout<typename P::S, L>;
+    constexpr int SMEM = NS * LY::STAGE_BYTES + NS * 8;
+    if (SMEM > 227 * 1024) return wt_set_error(WT_ERR_ARG, "streaming tile needs %d bytes of shared memory", SMEM);
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_step_stream<PREC, FAST, L, NS, THREADS, MINB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+            return wt_cuda_check("wt_step: shared-memory carve-out");
+        configured = true;
+    }
+    const auto& a = *static_cast<const StepArgs<typename P::S, typename P::T>*>(args);
+    const int32_t nchunks = (n + L - 1) / L;
+    const int32_t grid = std::min(nchunks, num_sms() * MINB);
+    k_step_stream<PREC, FAST, L, NS, THREADS, MINB><<<grid, THREADS, SMEM, st>>>(a);
+    return WT_OK;
+}
+
+#define WT_VARIANTS(PREC, FAST)                                                          \
+    {1, 0, 1, 256, 4, 0, 0, launch_bulk<PREC, FAST, 1, 256, 4>},                         \
+    {2, 0, 1, 128, 8, 0, 0, launch_bulk<PREC, FAST, 1, 128, 8>},                         \
+    {3, 0, 2, 128, 6, 0, 0, launch_bulk<PREC, FAST, 2, 128, 6>},                         \
+    {4, 0, 2, 128, 4, 0, 0, launch_bulk<PREC, FAST, 2, 128, 4>},                         \
+    {5, 0, 4, 128, 4, 0, 0, launch_bulk<PREC, FAST, 4, 128, 4>},                         \
+    {6, 0, 4, 128, 3, 0, 0, launch_bulk<PREC, FAST, 4, 128, 3>},                         \
+    {7, 0, 2, 256, 3, 0, 0, launch_bulk<PREC, FAST, 2, 256, 3>},                         \
+    {8, 1, 1, 1024, 1, 1024, 2, launch_stream<PREC, FAST, 1024, 2, 1024, 1>},            \
+    {9, 1, 1, 512, 2, 512, 2, launch_stream<PREC, FAST, 512, 2, 512, 2>},                \
+    {10, 1, 1, 512, 1, 512, 3, launch_stream<PREC, FAST, 512, 3, 512, 1>},               \
+    {11, 1, 1, 256, 2, 256, 4, launch_stream<PREC, FAST, 256, 4, 256, 2>},               \
+    {12, 1, 1, 1024, 1, 2048, 2, launch_stream<PREC, FAST, 2048, 2, 1024, 1>}
+
+template <int PREC, bool FAST>
+const StepVariant* variants(int* count) {
+    static const StepVariant table[] = {WT_VARIANTS(PREC, FAST)};
+    *count = (int)(sizeof(table) / sizeof(table[0]));
+    return table;
+}
+
+// defaults until the autotuner has measured the tunnel: one cell per thread at 64
+// registers; fp64 needs 128 registers to avoid spills, so two cells per thread there
+template <int PREC>
+const StepVariant* pick_variant(const wt_grid* g) {
+    int count;
+    const StepVariant* t = g->collision == WT_COLLIDE_FAST ? variants<PREC, true>(&count) : variants<PREC, false>(&count);
+    const int want = g->tile > 0 ? g->tile : (PREC == WT_F64 ? 4 : 1);
+    for (int k = 0; k < count; ++k) {
+        if (t[k].id != want) continue;
+        if (g->nx % t[k].v != 0) return nullptr;
+        if (PREC == WT_F64 && t[k].v == 4) return nullptr;
+        if (t[k].kind == 1 && g->nx % 16 != 0) return nullptr;  // 16-byte copies of rows and code bytes
+        return &t[k];
+    }
+    return nullptr;
 }
 
 template <int PREC>
 int step_impl(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
               cudaStream_t stream) {
-    using T = typename Prec<PREC>::T;
-    StepArgs<T> a;
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    using S = typename P::S;
+    StepArgs<S, T> a;
     a.solid = g->solid;
     a.code = g->code;
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
     a.nxy = g->nx * g->ny;
     a.n = a.nxy * g->nz;
     a.dnx = FastDiv((uint32_t)g->nx);
-    a.dnxy = FastDiv((uint32_t)a.nxy);
-    a.uin = (T)uin; a.tau = (T)tau; a.smag = (T)smag;
-    const unsigned nb_bulk = (unsigned)((a.n + 255) / 256);
-    const int32_t nface = a.nxy + a.nx * (a.nz - 2);
+    a.dny = FastDiv((uint32_t)g->ny);
+    a.dny2 = FastDiv((uint32_t)(g->ny - 2));
+    a.uin = (T)uin; a.tau = (T)tau;
+    const T sm = (T)smag;
+    a.csmag = (T)25.4558441 * sm * sm;  // same left-to-right product as server/lbm.py:152
+    const StepVariant* var = pick_variant<PREC>(g);
+    if (!var) return wt_set_error(WT_ERR_ARG, "wt_step: no kernel variant for tile %d (nx=%d)", g->tile, g->nx);
+    for (int b = 0; b < 2; ++b) {
+        const uintptr_t al = reinterpret_cast<uintptr_t>(g->f[b]);
+        if (al % 16 != 0) return wt_set_error(WT_ERR_ARG, "wt_step: population buffer %d not 16-byte aligned", b);
+    }
+    if (reinterpret_cast<uintptr_t>(g->code) % 16 != 0)
+        return wt_set_error(WT_ERR_ARG, "wt_step: code buffer not 16-byte aligned");
+    a.status = g->status;
+    a.test_skip_chunk = g->test_skip_chunk;
+    constexpr int VEC = 16 / (int)sizeof(S);
+    const int32_t nface = a.nxy + a.nx * (a.nz - 2) + (a.ny - 2) * (a.nz - 2);
     const unsigned nb_face = (unsigned)((nface + 255) / 256);
     for (int32_t s = 0; s < steps; ++s) {
-        a.fin = g->f[cur];
-        a.fout = g->f[cur ^ 1];
+        const S* fin = static_cast<const S*>(g->f[cur]);
+        S* fout = static_cast<S*>(g->f[cur ^ 1]);
+        for (int i = 0; i < Q; ++i) {
+            const int64_t off = cx(i) + (int64_t)cy(i) * a.nx + (int64_t)cz(i) * a.nxy;
+            a.src[i] = fin + (int64_t)i * a.n - off;
+            a.dst[i] = fout + (int64_t)i * a.n;
+            const int32_t r = (int32_t)(((-off) % VEC + VEC) % VEC);  // n and chunk starts are multiples of VEC
+            a.chunk_r[i] = r;
+            a.chunk_src[i] = a.src[i] - r;
+        }
+        a.fin = fin;
         a.mac_prev = static_cast<const T*>(g->mac[cur]);
         a.mac_cur = static_cast<T*>(g->mac[cur ^ 1]);
         a.mac_all = (flags & WT_STEP_MAC_ALL_LAST) && s == steps - 1;
-        k_step_bulk<PREC><<<nb_bulk, 256, 0, stream>>>(a);
+        if (int rc = var->launch(&a, a.n, stream)) return rc;
         k_step_faces<PREC><<<nb_face, 256, 0, stream>>>(a);
         cur ^= 1;
     }
@@ -362,6 +910,8 @@ extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin,
     if (cur != 0 && cur != 1) return wt_set_error(WT_ERR_ARG, "wt_step: cur must be 0 or 1");
     if (steps < 0) return wt_set_error(WT_ERR_ARG, "wt_step: steps < 0");
     if (steps == 0) return WT_OK;
+    if (g->collision != WT_COLLIDE_EXACT && g->collision != WT_COLLIDE_FAST)
+        return wt_set_error(WT_ERR_ARG, "wt_step: unknown collision form %d", g->collision);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch (g->precision) {
         case WT_F32: return wt::step_impl<WT_F32>(g, cur, steps, uin, tau, smag, flags, st);
@@ -370,4 +920,24 @@ extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin,
         case WT_F64: return wt::step_impl<WT_F64>(g, cur, steps, uin, tau, smag, flags, st);
         default: return wt_set_error(WT_ERR_ARG, "wt_step: unknown precision %d", g->precision);
     }
+}
+
+extern "C" int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap) {
+    int count = 0;
+    const wt::StepVariant* t = nullptr;
+    switch (precision) {
+        case WT_F32: t = wt::variants<WT_F32, false>(&count); break;
+        case WT_F16: t = wt::variants<WT_F16, false>(&count); break;
+        case WT_BF16: t = wt::variants<WT_BF16, false>(&count); break;
+        case WT_F64: t = wt::variants<WT_F64, false>(&count); break;
+        default: return wt_set_error(WT_ERR_ARG, "wt_step_tiles: unknown precision %d", precision);
+    }
+    for (int k = 0; k < count && k < cap; ++k) {
+        if (!out) break;
+        out[4 * k + 0] = t[k].id;
+        out[4 * k + 1] = t[k].kind == 0 ? t[k].v : -t[k].chunk;  // negative: streaming chunk length
+        out[4 * k + 2] = t[k].block;
+        out[4 * k + 3] = t[k].kind == 0 ? t[k].minb : t[k].stages;
+    }
+    return count;
 }

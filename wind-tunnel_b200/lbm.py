@@ -65,12 +65,14 @@ class Solver:
     """One tunnel. Method-for-method the reference Solver (server/lbm.py:398-482).
 
     Extra keyword arguments: ``precision`` ('fp32' as the reference, 'fp16'/'bf16' for
-    shifted half-width population storage, 'fp64' for the oracle run), ``stream`` (a
-    ``torch.cuda.Stream``; by default each Solver owns one) and ``seed`` (particle
-    initialisation; the reference draws from an unseeded generator).
+    shifted half-width population storage, 'fp64' for the oracle run), ``collision``
+    ('exact' reference operation order or 'fast' moment-space form; by default exact for
+    fp32/fp64 and fast for fp16/bf16), ``stream`` (a ``torch.cuda.Stream``; by default each
+    Solver owns one) and ``seed`` (particle initialisation; the reference draws from an
+    unseeded generator).
     """
 
-    def __init__(self, dims, device=None, precision='fp32', stream=None, seed=None):
+    def __init__(self, dims, device=None, precision='fp32', stream=None, seed=None, collision=None):
         self.dev = _device(device)
         self.nx, self.ny, self.nz = (int(d) for d in dims)
         self.n = n = self.nx * self.ny * self.nz
@@ -78,6 +80,13 @@ class Solver:
         self.precision = W.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         if self.precision not in _TORCH_POP:
             raise ValueError(f'unknown precision {precision!r}')
+        # 'exact': the reference's expressions in its order (default for fp32/fp64, the
+        # drop-in form); 'fast': the moment-space form (default for fp16/bf16 storage)
+        if collision is None:
+            collision = 'fast' if self.precision in (W.F16, W.BF16) else 'exact'
+        if collision not in ('exact', 'fast'):
+            raise ValueError(f'unknown collision form {collision!r}')
+        self.collision = collision
         self.stream = stream if stream is not None else torch.cuda.Stream(self.dev)
         mac_dt = torch.float64 if self.precision == W.F64 else torch.float32
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
@@ -88,6 +97,7 @@ class Solver:
             self.code = torch.zeros(n, dtype=torch.uint8, device=self.dev)
             self.forces_dev = torch.zeros(6, dtype=torch.float64, device=self.dev)
             self.mass_dev = torch.zeros(1, dtype=torch.float64, device=self.dev)
+            self.status_dev = torch.zeros(1, dtype=torch.int32, device=self.dev)
             self.partials = torch.empty(int(W.lib().wt_reduce_scratch_len(0)), dtype=torch.float64, device=self.dev)
             self.slice_max = max(self.nx * self.ny, self.nx * self.nz, self.nz * self.ny)
             self.slice_buf = torch.zeros(self.slice_max * 2, dtype=torch.uint8, device=self.dev)
@@ -97,7 +107,9 @@ class Solver:
         self.grid = W.Grid(self.nx, self.ny, self.nz, self.precision,
                            (ctypes.c_void_p * 2)(self.f[0].data_ptr(), self.f[1].data_ptr()),
                            (ctypes.c_void_p * 2)(self.mac[0].data_ptr(), self.mac[1].data_ptr()),
-                           self.solid.data_ptr(), self.code.data_ptr())
+                           self.solid.data_ptr(), self.code.data_ptr(), 0,
+                           W.COLLIDE_FAST if collision == 'fast' else W.COLLIDE_EXACT)
+        self.grid.status = self.status_dev.data_ptr()
         self.gp = ctypes.byref(self.grid)
         self.sh = W.stream_handle(self.stream)
         self.cur = 0
@@ -108,6 +120,14 @@ class Solver:
         self._host = {}
         self._pending = None
         self.stream.synchronize()
+
+    def set_tile(self, tile):
+        """Select a step-kernel tile variant (see wtlib.step_tiles; 0 = library default)."""
+        self.grid.tile = int(tile)
+
+    @property
+    def tile(self):
+        return int(self.grid.tile)
 
     # ---- set-up (server/lbm.py:415-440) ----
     def reset(self, uin):
@@ -280,6 +300,16 @@ class Solver:
 
     def synchronize(self):
         self.stream.synchronize()
+
+    def status(self, clear=True):
+        """Device status word: 0, or wtlib.WT_ERR_TIMEOUT if a kernel's bounded wait gave up
+        (the populations are then invalid until the next reset)."""
+        self.stream.synchronize()
+        v = int(self.status_dev.cpu()[0])
+        if clear and v:
+            self.status_dev.zero_()
+            torch.cuda.synchronize(self.dev)
+        return v
 
 
 def _weights():

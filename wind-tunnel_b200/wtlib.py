@@ -15,10 +15,11 @@ WT_OK, WT_ERR_ARG, WT_ERR_DIMS, WT_ERR_CUDA, WT_ERR_CAPACITY, WT_ERR_TIMEOUT = 0
 F32, F16, BF16, F64 = 0, 1, 2, 3
 PRECISIONS = {'fp32': F32, 'fp16': F16, 'bf16': BF16, 'fp64': F64}
 STEP_MAC_ALL_LAST = 1
+COLLIDE_EXACT, COLLIDE_FAST = 0, 1
 
 # every symbol include/wt.h declares (tests check that the library exports them all)
 EXPORTS = ['wt_last_error', 'wt_abi_version', 'wt_check_dims', 'wt_population_bytes', 'wt_init_eq',
-           'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step',
+           'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step_tiles', 'wt_step',
            'wt_reduce_scratch_len', 'wt_forces', 'wt_mass', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp']
 
 
@@ -33,7 +34,9 @@ class Grid(ctypes.Structure):
     _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32),
                 ('precision', ctypes.c_int32),
                 ('f', ctypes.c_void_p * 2), ('mac', ctypes.c_void_p * 2),
-                ('solid', ctypes.c_void_p), ('code', ctypes.c_void_p)]
+                ('solid', ctypes.c_void_p), ('code', ctypes.c_void_p),
+                ('tile', ctypes.c_int32), ('collision', ctypes.c_int32),
+                ('status', ctypes.c_void_p), ('test_skip_chunk', ctypes.c_int32), ('pad_', ctypes.c_int32)]
 
 
 _lib = None
@@ -58,6 +61,7 @@ def lib():
             'wt_links_scratch_len': ([i64], i64),
             'wt_links_scan': ([gp, vp, vp, vp], ctypes.c_int),
             'wt_links_fill': ([gp, vp, vp, vp, i64, vp], ctypes.c_int),
+            'wt_step_tiles': ([i32, vp, i32], ctypes.c_int),
             'wt_step': ([gp, i32, i32, f64, f64, f64, i32, vp], ctypes.c_int),
             'wt_reduce_scratch_len': ([i64], i64),
             'wt_forces': ([gp, i32, vp, vp, i64, vp, vp, vp], ctypes.c_int),
@@ -89,6 +93,15 @@ def call(name, *args):
 def ptr(t):
     """Raw device (or host) address of a tensor, or None."""
     return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def step_tiles(precision):
+    """[(id, cells_per_thread, threads_per_block, min_blocks_per_sm), ...] of the step kernel."""
+    buf = (ctypes.c_int32 * 256)()
+    n = lib().wt_step_tiles(int(precision), buf, 64)
+    if n < 0:
+        check(n)
+    return [tuple(buf[4 * k:4 * k + 4]) for k in range(n)]
 
 
 def stream_handle(stream):
