@@ -239,29 +239,38 @@ def test_autotune_picks_a_tile():
     assert tile in ms and s.tile == tile and all(v > 0 for v in ms.values())
 
 
+# The fast form takes reciprocals and square roots from the special-function unit (about
+# 1 float ulp), the oracle restates the same algebra with IEEE operations; after 5 steps
+# the populations must agree to these absolute tolerances (f is O(0.03..0.33)):
+FAST_ATOL = {'fp32': 2e-6, 'fp16': 3e-5, 'bf16': 3e-4, 'fp64': 1e-12}
+
+
 @pytest.mark.parametrize('prec_name,oprec', [('fp32', 0), ('fp16', 1), ('bf16', 2), ('fp64', 3)])
 @pytest.mark.parametrize('dims', [(64, 24, 20), (34, 9, 7)])
 def test_fast_collision_matches_oracle(oracle_mod, prec_name, oprec, dims):
-    """The moment-space collision, every storage precision, bit-exact against the oracle's
+    """The moment-space collision in every storage precision and tile against the oracle's
     restatement of the same operation sequence."""
+    import autotune
     solid = _random_case(dims, 23)
     uin, tau, smag = 0.07, 0.515, 0.16
-    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name, collision='fast')
-    s.reset(uin)
     L = oracle_mod.Lattice(dims, oprec, collision=1)
     L.solid[:] = solid
     L.reset(uin)
+    L.step(5, uin, tau, smag)
+    ref = L.populations()
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name, collision='fast')
     p = dict(uIn=uin, tau=tau, smag=smag)
-    import autotune
-    for tile in autotune.admissible(s)[:4]:
+    tiles = autotune.admissible(s)
+    assert tiles
+    for tile in tiles:
         s.set_tile(tile[0])
-        s.step(3, p)
-        L.step(3, uin, tau, smag)
-        s.synchronize()
-        dev = s.f[s.cur].cpu()
-        dev = dev.view(torch.int16).numpy().view(np.uint16) if oprec == 2 else dev.numpy()
-        assert np.array_equal(dev, L.f[L.cur]), f'{prec_name} tile {tile}'
-        assert np.array_equal(s.mac[s.cur].cpu().numpy(), L.mac), f'{prec_name} tile {tile}'
+        s.reset(uin)
+        s.cur = 0
+        s.step(5, p)
+        got = s.populations()
+        err = np.abs(got - ref).max()
+        assert err <= FAST_ATOL[prec_name], f'{prec_name} tile {tile}: max |df| {err}'
+        np.testing.assert_allclose(s.macro(), L.mac.astype(np.float64), atol=20 * FAST_ATOL[prec_name], rtol=0)
 
 
 def test_fast_collision_close_to_exact():

@@ -56,7 +56,7 @@ def admissible(solver):
             continue
         if v < 0:
             chunk, stages = -v, t[3]
-            smem = stages * (19 * (chunk + 16 // elem) * elem + chunk) + 8 * stages
+            smem = stages * (19 * (chunk + 16 // elem) * elem + chunk) + 16 * stages
             if solver.nx % 16 or smem > SMEM_LIMIT:
                 continue
         out.append(t)

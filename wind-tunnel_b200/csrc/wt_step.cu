@@ -294,7 +294,31 @@ __device__ __forceinline__ double fmaT(double a, double b, double c) { return __
 // term. About 200 floating-point operations per cell against 330 in the reference order.
 // With SHIFT the inputs and outputs are deviations v_i = f_i - w_i (the fp16/bf16 storage
 // form): the constant parts cancel analytically, which keeps small numbers small.
-// Every operation is an IEEE add/mul/fma/div/sqrt, so the oracle reproduces it exactly.
+// Reciprocals and square roots use the special-function unit (rcp_fast etc.), so results
+// match the oracle's IEEE restatement of this form to within a few float ulps.
+// Reciprocal and square roots for the fast form: the special-function unit's
+// approximation refined by one Newton step (about 1 ulp in float); IEEE ops in double.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    const float e = __fmaf_rn(-x, r, 1.0f);
+    return __fmaf_rn(r, e, r);
+}
+__device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
+__device__ __forceinline__ float sqrt_fast(float x) {  // x >= 0 (0 maps to 0)
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
+__device__ __forceinline__ float rsqrt_fast(float x) {  // x > 0
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    const float h = __fmul_rn(__fmul_rn(0.5f, x), __fmul_rn(r, r));
+    return __fmul_rn(r, __fsub_rn(1.5f, h));
+}
+__device__ __forceinline__ double rsqrt_fast(double x) { return 1.0 / sqrt(x); }
+
 template <class T, bool SHIFT>
 __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy,
                                              T& ouz, T& orho) {
@@ -315,11 +339,11 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
     const T jy = ((a3 + a7) - (a9 - a15)) + a17;
     const T jz = ((a5 + a11) - (a13 - a15)) - a17;
     const T rho = SHIFT ? S + (T)1.0 : S;
-    const T ir = (T)1.0 / rho;
+    const T ir = rcp_fast(rho);
     T ux = jx * ir, uy = jy * ir, uz = jz * ir;
     T usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
     if (usq > (T)0.1225) {  // |u| > 0.35 (server/lbm.py:131-135)
-        const T sc = (T)0.35 / sqrt(usq);
+        const T sc = (T)0.35 * rsqrt_fast(usq);
         ux = ux * sc; uy = uy * sc; uz = uz * sc;
         usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
     }
@@ -329,12 +353,12 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
     const T nxy = fmaT(-rux, uy, xxy), nxz = fmaT(-rux, uz, xxz), nyz = fmaT(-ruy, uz, xyz);
     const T q1 = fmaT(nzz, nzz, fmaT(nyy, nyy, nxx * nxx));
     const T q2 = fmaT(nyz, nyz, fmaT(nxz, nxz, nxy * nxy));
-    const T qn = sqrt(fmaT((T)2.0, q2, q1));
+    const T qn = sqrt_fast(fmaT((T)2.0, q2, q1));
     T tau0 = tau;
     const T sp = (T)x - (T)(nx - 24);  // outlet sponge (server/lbm.py:149-151)
     if (sp > (T)0.0) tau0 = fmaT(sp, (T)0.015, tau);
-    const T tau_e = (T)0.5 * (tau0 + sqrt(fmaT(tau0, tau0, csmag * qn * ir)));
-    const T keep = (T)1.0 - (T)1.0 / tau_e;
+    const T tau_e = (T)0.5 * (tau0 + sqrt_fast(fmaT(tau0, tau0, csmag * qn * ir)));
+    const T keep = (T)1.0 - rcp_fast(tau_e);
     const T k45 = (T)4.5 * keep, k9 = (T)9.0 * keep;
     const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
     const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;  // 2 A_ab
@@ -406,6 +430,7 @@ __device__ __forceinline__ typename P::T ld_in(const typename P::S* p) {
     if constexpr (FAST) return P::to(*p);
     else return ld_pop<P, I>(p);
 }
+
 template <class P, bool FAST, int I>
 __device__ __forceinline__ void st_out(typename P::S* p, typename P::T v) {
     if constexpr (FAST) *p = P::from(v);
@@ -603,11 +628,16 @@ __global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec
 // contiguous source range src[i][c0 .. c0 + L): every population of a chunk of cells is
 // one 1-D bulk copy (cp.async.bulk, no tensor map, no multicast). The copy starts at the
 // 16-byte boundary at or below the range (chunk_src[i] = src[i] - chunk_r[i]) and is one
-// vector longer, so the cell at chunk offset c is stage[i][chunk_r[i] + c]. One elected
-// thread issues the 19 population copies plus the chunk's code bytes into a stage and
-// arms its mbarrier with the byte count; all threads wait on the barrier (bounded), update
-// the chunk from shared memory and store to global memory, then the stage is refilled
-// with the chunk S positions ahead. Persistent CTAs walk chunks blockIdx.x + j*gridDim.x.
+// vector longer, so the cell at chunk offset c is stage[i][chunk_r[i] + c].
+//
+// Warp-specialised pipeline of NS stages per CTA: warp 0 is the producer (one lane issues
+// the 19 population copies and the chunk's code bytes into a free stage and arms the
+// stage's "full" mbarrier with the byte count); the other warps consume (wait on "full",
+// update their cells from shared memory, store to global memory, then arrive on the
+// stage's "empty" mbarrier). There is no CTA-wide barrier in the loop, so a consumer warp
+// slowed by boundary cells does not hold the others back. Persistent CTAs walk chunks
+// blockIdx.x + j*gridDim.x. Every wait is bounded; a wait that gives up sets the tunnel's
+// status word to WT_ERR_TIMEOUT and the warp leaves.
 // ---------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -619,24 +649,27 @@ __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// try_wait suspends the thread until the phase completes or ~SUSPEND_NS elapse
+constexpr uint32_t SUSPEND_NS = 1000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "n"(SUSPEND_NS)
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after about a second (each try_wait may itself suspend briefly).
+// Bounded wait: gives up after WAIT_LIMIT tries, about a second.
 constexpr uint32_t WAIT_LIMIT = 1u << 20;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
         if (mbar_try_wait(bar, parity)) return true;
-        if (it > 32) __nanosleep(256);
-    }
     return false;
 }
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -645,6 +678,76 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+template <class S>
+__device__ __forceinline__ S lds(const S* p) {
+    static_assert(sizeof(S) == 1 || sizeof(S) == 2 || sizeof(S) == 4 || sizeof(S) == 8, "lds width");
+    const uint32_t a = smem_u32(p);
+    if constexpr (sizeof(S) == 1) {
+        unsigned short v;
+        asm volatile("ld.shared.u8 %0, [%1];" : "=h"(v) : "r"(a));
+        return (S)v;
+    } else if constexpr (sizeof(S) == 4) {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+        return *reinterpret_cast<S*>(&v);
+    } else if constexpr (sizeof(S) == 2) {
+        unsigned short v;
+        asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+        return *reinterpret_cast<S*>(&v);
+    } else {
+        double v;
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+        return *reinterpret_cast<S*>(&v);
+    }
+}
+template <class S>
+__device__ __forceinline__ void sts(S* p, S v) {
+    static_assert(sizeof(S) == 2 || sizeof(S) == 4 || sizeof(S) == 8, "sts width");
+    const uint32_t a = smem_u32(p);
+    if constexpr (sizeof(S) == 4) {
+        asm volatile("st.shared.b32 [%0], %1;" ::"r"(a), "r"(*reinterpret_cast<uint32_t*>(&v)) : "memory");
+    } else if constexpr (sizeof(S) == 2) {
+        asm volatile("st.shared.b16 [%0], %1;" ::"r"(a), "h"(*reinterpret_cast<unsigned short*>(&v)) : "memory");
+    } else {
+        asm volatile("st.shared.b64 [%0], %1;" ::"r"(a), "l"(*reinterpret_cast<unsigned long long*>(&v)) : "memory");
+    }
+}
+
+template <class S>
+__device__ __forceinline__ SVec<S, 2> lds_pair(const S* p) {  // p aligned to 2 elements
+    SVec<S, 2> r;
+    const uint32_t a = smem_u32(p);
+    if constexpr (sizeof(S) == 2) {
+        uint32_t v;
+        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
+        memcpy(&r, &v, 4);
+    } else if constexpr (sizeof(S) == 4) {
+        uint2 v;
+        asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+        memcpy(&r, &v, 8);
+    } else {
+        uint4 v;
+        asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+        memcpy(&r, &v, 16);
+    }
+    return r;
+}
+// the same from a shared-memory stage
+template <class P, bool FAST, int I>
+__device__ __forceinline__ typename P::T ld_in_smem(const typename P::S* p) {
+    const typename P::S v = lds(p);
+    return ld_in<P, FAST, I>(&v);
 }
 
 template <class S, int L>
@@ -656,108 +759,149 @@ struct StreamLayout {
     static_assert(L % 16 == 0, "chunk length");
 };
 
-template <int PREC, int L, int NS>
-__device__ __forceinline__ void stream_issue(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
-                                             unsigned char* smem, uint64_t* bar, int32_t chunk, int st) {
+template <int PREC, int L>
+__device__ __forceinline__ bool stream_issue(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                             unsigned char* stage, uint64_t* full, int32_t chunk) {
     using S = typename Prec<PREC>::S;
     using LY = StreamLayout<S, L>;
-    if (chunk + 1 == a.test_skip_chunk) return;  // test hook: leave the stage empty
+    if (chunk + 1 == a.test_skip_chunk) return false;  // test hook: leave the stage empty
     const int32_t c0 = chunk * L;
     const int32_t len = min(L, a.n - c0);
     const int32_t len16 = (len + LY::VEC - 1) / LY::VEC * LY::VEC;
     const uint32_t pop_bytes = (uint32_t)((len16 + LY::VEC) * (int)sizeof(S));
     const uint32_t code_bytes = (uint32_t)((len + 15) / 16 * 16);
-    unsigned char* stage = smem + (size_t)st * LY::STAGE_BYTES;
-    mbar_arrive_expect_tx(&bar[st], Q * pop_bytes + code_bytes);
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(full, Q * pop_bytes + code_bytes);
 #pragma unroll 1
-    for (int i = 0; i < Q; ++i) bulk_g2s(stage + i * LY::POP_BYTES, a.chunk_src[i] + c0, pop_bytes, &bar[st]);
-    bulk_g2s(stage + Q * LY::POP_BYTES, a.code + c0, code_bytes, &bar[st]);
+    for (int i = 0; i < Q; ++i) bulk_g2s(stage + i * LY::POP_BYTES, a.chunk_src[i] + c0, pop_bytes, full);
+    bulk_g2s(stage + Q * LY::POP_BYTES, a.code + c0, code_bytes, full);
+    return true;
 }
 
-template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB>
+template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB, int CPT>
 __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
     using P = Prec<PREC>;
     using T = typename P::T;
     using S = typename P::S;
     using LY = StreamLayout<S, L>;
+    constexpr int CONSUMERS = THREADS / 32 - 1;  // consumer warps
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NS * LY::STAGE_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + NS * LY::STAGE_BYTES);
+    uint64_t* empty = full + NS;
     const int32_t nchunks = (a.n + L - 1) / L;
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < NS; ++st) mbar_init(&bar[st], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    uint32_t inflight = 0;  // thread 0: stages with a copy issued and not yet consumed
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         for (int st = 0; st < NS; ++st) {
-            const int32_t k = blockIdx.x + st * gridDim.x;
-            if (k < nchunks) {
-                stream_issue<PREC, L, NS>(a, smem, bar, k, st);
-                inflight |= 1u << st;
-            }
+            mbar_init(&full[st], 1);
+            mbar_init(&empty[st], CONSUMERS);
         }
+        mbar_fence_init();
     }
+    __syncthreads();  // the only CTA-wide barrier: barriers initialised
+
+    if (warp == 0) {
+        // ---- producer ----
+        if (lane != 0) return;
+        int32_t issued_lo = 0, j = 0;  // chunks [issued_lo, j) issued and possibly unconsumed
+        for (;; ++j) {
+            const int32_t k = blockIdx.x + j * gridDim.x;
+            if (k >= nchunks) break;
+            const int st = j % NS;
+            if (j >= NS) {
+                if (!mbar_wait(&empty[st], (uint32_t)(((j / NS) - 1) & 1))) {
+                    if (a.status) atomicExch(a.status, WT_ERR_TIMEOUT);
+                    break;
+                }
+                issued_lo = j - NS + 1;
+            }
+            if (!stream_issue<PREC, L>(a, smem + (size_t)st * LY::STAGE_BYTES, &full[st], k)) continue;
+        }
+        // keep the CTA's shared memory alive until every issued copy has landed (bounded)
+        for (int32_t q = issued_lo; q < j; ++q) {
+            const int32_t k = blockIdx.x + q * gridDim.x;
+            if (k + 1 == a.test_skip_chunk) continue;
+            mbar_wait(&full[q % NS], (uint32_t)((q / NS) & 1));
+        }
+        return;
+    }
+
+    // ---- consumers ----
+    // Consumer thread ct owns CPT consecutive cells of each chunk (L = 32 * CONSUMERS * CPT),
+    // so a warp reads and writes contiguous runs; with CPT = 2 loads and stores are pairs.
+    static_assert(L == 32 * CONSUMERS * CPT, "chunk = consumer threads x cells per thread");
+    const int ct = threadIdx.x - 32;
+    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
 #pragma unroll 1
     for (int32_t j = 0;; ++j) {
         const int32_t k = blockIdx.x + j * gridDim.x;
         if (k >= nchunks) break;
         const int st = j % NS;
-        const uint32_t parity = (uint32_t)((j / NS) & 1);
-        const bool ok = mbar_wait(&bar[st], parity);
-        if (__syncthreads_or(!ok)) {  // one decision for the whole CTA
-            // the stage never filled: report, drain the copies this CTA still has in flight
-            // (bounded), and leave; the tunnel's state is invalid until the next reset
-            if (a.status && threadIdx.x == 0) atomicExch(a.status, WT_ERR_TIMEOUT);
-            if (threadIdx.x == 0) {
-                for (int d = 1; d < NS; ++d) {
-                    const int s2 = (st + d) % NS;
-                    const int32_t j2 = j + d;
-                    if ((inflight >> s2) & 1u) mbar_wait(&bar[s2], (uint32_t)((j2 / NS) & 1));
-                }
-            }
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((j / NS) & 1)))) {
+            // the stage never filled: report and leave (the tunnel is invalid until reset)
+            if (a.status && lane == 0) atomicExch(a.status, WT_ERR_TIMEOUT);
             return;
         }
         const unsigned char* stage = smem + (size_t)st * LY::STAGE_BYTES;
         const uint8_t* codes = stage + Q * LY::POP_BYTES;
         const int32_t c0 = k * L;
         const int32_t len = min(L, a.n - c0);
-#pragma unroll 1
-        for (int32_t c = threadIdx.x; c < len; c += THREADS) {
+        const int32_t c = ct * CPT;
+        if (c < len) {  // len is a multiple of 16, so all CPT cells are in range
             const int32_t idx = c0 + c;
             const int32_t row = (int32_t)a.dnx.div((uint32_t)idx);
-            const int32_t x = idx - row * nx;
+            const int32_t x = idx - row * nx;  // nx is a multiple of CPT: the cells share the row
             const int32_t z = (int32_t)a.dny.div((uint32_t)row);
             const int32_t y = row - z * ny;
             const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
             const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-            const uint32_t code = codes[c];
-            if (!face_row && x > 0 && x < nx - 1 && code == 0) {
-                T f[Q];
+            uint32_t code;
+            if constexpr (CPT == 1) code = lds(codes + c);
+            else code = lds(reinterpret_cast<const uint16_t*>(codes + c));
+            if (!face_row && x > 0 && x + CPT < nx && code == 0) {
+                T f[CPT][Q];
                 unroll<0, Q>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
                     const S* sp = reinterpret_cast<const S*>(stage + i * LY::POP_BYTES) + a.chunk_r[i] + c;
-                    f[i] = ld_in<P, FAST, i>(sp);
+                    if constexpr (CPT == 1) {
+                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
+                    } else if constexpr (cx(i) == 0) {  // chunk_r[i] == 0: an aligned pair
+                        const SVec<S, 2> v = lds_pair(sp);
+                        f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
+                        f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
+                    } else {
+                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
+                        f[1][i] = ld_in_smem<P, FAST, i>(sp + 1);
+                    }
                 });
-                T ux, uy, uz, rho;
-                collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, ux, uy, uz, rho);
-                store_cell<P, FAST>(a, idx, f);
-                if (a.mac_all || row_shell || x == 1 || x == nx - 2) store_mac(a.mac_cur, idx, ux, uy, uz, rho);
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    T ux, uy, uz, rho;
+                    collide_any<P, FAST>(f[q], x + q, nx, a.tau, a.csmag, ux, uy, uz, rho);
+                    if (a.mac_all || row_shell || x + q == 1 || x + q == nx - 2)
+                        store_mac(a.mac_cur, idx + q, ux, uy, uz, rho);
+                }
+                unroll<0, Q>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    if constexpr (CPT == 1) {
+                        st_out<P, FAST, i>(a.dst[i] + idx, f[0][i]);
+                    } else {
+                        SVec<S, 2> v;
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            if constexpr (P::shifted && !FAST) v.v[q] = P::from(f[q][i] - (T)wd(i));
+                            else v.v[q] = P::from(f[q][i]);
+                        }
+                        vstore<S, 2>(a.dst[i] + idx, v);
+                    }
+                });
             } else {
-                general_cell<P, FAST>(a, idx, x, y, z, code, face_row, row_shell);
+#pragma unroll 1
+                for (int q = 0; q < CPT; ++q)
+                    general_cell<P, FAST>(a, idx + q, x + q, y, z, (code >> (8 * q)) & 0xffu, face_row, row_shell);
             }
         }
-        __syncthreads();  // every thread is done with this stage
-        if (threadIdx.x == 0) {
-            inflight &= ~(1u << st);
-            const int32_t kn = k + NS * gridDim.x;
-            if (kn < nchunks) {
-                fence_proxy_async_smem();
-                stream_issue<PREC, L, NS>(a, smem, bar, kn, st);
-                inflight |= 1u << st;
-            }
-        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[st]);  // this warp is done with the stage
     }
 }
 
@@ -789,15 +933,15 @@ static int launch_bulk(const void* args, int32_t n, cudaStream_t st) {
     return WT_OK;
 }
 
-template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB>
+template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB, int CPT>
 static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     using P = Prec<PREC>;
     using LY = StreamLayout<typename P::S, L>;
-    constexpr int SMEM = NS * LY::STAGE_BYTES + NS * 8;
+    constexpr int SMEM = NS * LY::STAGE_BYTES + 2 * NS * 8;
     if (SMEM > 227 * 1024) return wt_set_error(WT_ERR_ARG, "streaming tile needs %d bytes of shared memory", SMEM);
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(k_step_stream<PREC, FAST, L, NS, THREADS, MINB>,
+        if (cudaFuncSetAttribute(k_step_stream<PREC, FAST, L, NS, THREADS, MINB, CPT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
             return wt_cuda_check("wt_step: shared-memory carve-out");
         configured = true;
@@ -805,7 +949,7 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     const auto& a = *static_cast<const StepArgs<typename P::S, typename P::T>*>(args);
     const int32_t nchunks = (n + L - 1) / L;
     const int32_t grid = std::min(nchunks, num_sms() * MINB);
-    k_step_stream<PREC, FAST, L, NS, THREADS, MINB><<<grid, THREADS, SMEM, st>>>(a);
+    k_step_stream<PREC, FAST, L, NS, THREADS, MINB, CPT><<<grid, THREADS, SMEM, st>>>(a);
     return WT_OK;
 }
 
@@ -817,11 +961,12 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     {5, 0, 4, 128, 4, 0, 0, launch_bulk<PREC, FAST, 4, 128, 4>},                         \
     {6, 0, 4, 128, 3, 0, 0, launch_bulk<PREC, FAST, 4, 128, 3>},                         \
     {7, 0, 2, 256, 3, 0, 0, launch_bulk<PREC, FAST, 2, 256, 3>},                         \
-    {8, 1, 1, 1024, 1, 1024, 2, launch_stream<PREC, FAST, 1024, 2, 1024, 1>},            \
-    {9, 1, 1, 512, 2, 512, 2, launch_stream<PREC, FAST, 512, 2, 512, 2>},                \
-    {10, 1, 1, 512, 1, 512, 3, launch_stream<PREC, FAST, 512, 3, 512, 1>},               \
-    {11, 1, 1, 256, 2, 256, 4, launch_stream<PREC, FAST, 256, 4, 256, 2>},               \
-    {12, 1, 1, 1024, 1, 2048, 2, launch_stream<PREC, FAST, 2048, 2, 1024, 1>}
+    {8, 1, 1, 512, 2, 480, 3, launch_stream<PREC, FAST, 480, 3, 512, 2, 1>},             \
+    {9, 1, 1, 512, 2, 480, 2, launch_stream<PREC, FAST, 480, 2, 512, 2, 1>},             \
+    {10, 1, 1, 1024, 1, 992, 2, launch_stream<PREC, FAST, 992, 2, 1024, 1, 1>},          \
+    {11, 1, 2, 512, 1, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 1, 2>},            \
+    {12, 1, 1, 512, 2, 480, 4, launch_stream<PREC, FAST, 480, 4, 512, 2, 1>},            \
+    {13, 1, 2, 512, 2, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 2, 2>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants(int* count) {
