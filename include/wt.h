@@ -121,6 +121,19 @@ int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau
 int64_t wt_reduce_scratch_len(int64_t count);
 int wt_forces(const wt_grid* g, int32_t cur, const int32_t* cells, const uint32_t* masks, int64_t n_links,
               double* partials, double* out6, void* stream);
+/* wt_forces without caller scratch. No counterpart in the reference: it exists for callers
+ * that cannot allocate device memory on the call path (a host framework that owns the
+ * device memory pool and passes only inputs and outputs, or a per-frame loop where an
+ * allocation would synchronise the device). The block partials live in a 192 KB array
+ * compiled into libwt.so, held by every GPU that loads the library until exit. At most
+ * WT_NOALLOC_MAX_LINKS link cells per call (WT_ERR_CAPACITY beyond). The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture. All calls share the array: calls whose kernels overlap on the
+ * GPU race and must not be issued. Results equal wt_forces to fp64 rounding (the blocks
+ * partition the list differently). */
+#define WT_NOALLOC_MAX_LINKS 1048576
+int wt_forces_noalloc(const wt_grid* g, int32_t cur, const int32_t* cells, const uint32_t* masks, int64_t n_links,
+                      double* out6, void* stream);
 /* Total mass sum_{fluid cells} sum_i f_i of f[cur] in double, deterministic. */
 int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void* stream);
 

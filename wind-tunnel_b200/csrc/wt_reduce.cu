@@ -8,6 +8,8 @@
 // fixed stride of the list, a fixed shuffle tree per warp and block, and a second one-block
 // pass over the block partials. The order never depends on scheduling, so repeated runs
 // are bit-identical.
+#include <mutex>
+
 #include "wt_common.cuh"
 
 namespace wt {
@@ -46,7 +48,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_force_partial(const typename Pr
     using P = Prec<PREC>;
     using T = typename P::T;
     double acc[FORCE_VALS] = {0, 0, 0, 0, 0, 0};
-    for (int64_t k = blockIdx.x * (int64_t)RED_THREADS + threadIdx.x; k < count; k += (int64_t)RED_BLOCKS * RED_THREADS) {
+    for (int64_t k = blockIdx.x * (int64_t)RED_THREADS + threadIdx.x; k < count; k += (int64_t)gridDim.x * RED_THREADS) {
         const int32_t idx = cells[k];
         const uint32_t m = masks[k];
         const int32_t z = (int32_t)dnxy.div((uint32_t)idx);
@@ -173,5 +175,84 @@ extern "C" int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* 
         case WT_BF16: return mass_impl<WT_BF16>(g, cur, partials, out1, st);
         case WT_F64: return mass_impl<WT_F64>(g, cur, partials, out1, st);
         default: return wt_set_error(WT_ERR_ARG, "wt_mass: unknown precision %d", g->precision);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Forces without caller-provided scratch.
+//
+// Some callers cannot allocate device memory on the call path: a host framework that owns
+// the device's memory pool and hands this library only its input and output buffers
+// (a plugin), or a per-frame serving loop where a cudaMalloc/cudaFree pair would
+// synchronise the device and stall every tunnel sharing the GPU. For them the block
+// partials of the force reduction live in the array below, compiled into the library:
+// every GPU that loads libwt.so holds these 192 KB until the process exits.
+//
+// Limits and sharing: one block of RED_THREADS threads per RED_THREADS link cells, so at
+// most NOALLOC_MAX_BLOCKS * RED_THREADS = 1,048,576 link cells per call; longer lists are
+// rejected with WT_ERR_CAPACITY. Every call on a device uses the same array and it keeps
+// the last call's contents. Nothing has to start at zero: each call writes every partial
+// it then reads. Calls whose kernels overlap on the GPU (different streams, no ordering
+// between them) race on the array and must not be issued.
+// ---------------------------------------------------------------------------------------
+constexpr int NOALLOC_MAX_BLOCKS = 4096;
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_BLOCKS * FORCE_VALS];
+
+// Device address of g_noalloc_partials for the current device, looked up once per device
+// (the host-side symbol is only a stand-in and must never be passed to a kernel).
+static int noalloc_scratch(double** out) {
+    static std::mutex mu;
+    static double* addr[128] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+        return wt_set_error(WT_ERR_CUDA, "wt_forces_noalloc: no current CUDA device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || !p)
+            return wt_set_error(WT_ERR_CUDA, "wt_forces_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        addr[dev] = static_cast<double*>(p);
+    }
+    *out = addr[dev];
+    return WT_OK;
+}
+
+template <int PREC>
+static int forces_noalloc_impl(const wt_grid* g, int32_t cur, const int32_t* cells, const uint32_t* masks,
+                               int64_t count, double* partials, double* out6, cudaStream_t st) {
+    using S = typename Prec<PREC>::S;
+    const int32_t nxy = g->nx * g->ny;
+    const int64_t n = (int64_t)nxy * g->nz;
+    const int nb = (int)((count + RED_THREADS - 1) / RED_THREADS);
+    if (nb > 0)
+        k_force_partial<PREC><<<nb, RED_THREADS, 0, st>>>(static_cast<const S*>(g->f[cur]), cells, masks, count, n,
+                                                           g->nx, nxy, FastDiv((uint32_t)g->nx), FastDiv((uint32_t)nxy),
+                                                           partials);
+    k_final<FORCE_VALS><<<1, RED_THREADS, 0, st>>>(partials, nb, out6);
+    return wt_cuda_check("wt_forces_noalloc launch");
+}
+
+extern "C" int wt_forces_noalloc(const wt_grid* g, int32_t cur, const int32_t* cells, const uint32_t* masks,
+                                 int64_t n_links, double* out6, void* stream) {
+    if (n_links > (int64_t)NOALLOC_MAX_BLOCKS * RED_THREADS)
+        return wt_set_error(WT_ERR_CAPACITY,
+                            "wt_forces_noalloc: %lld link cells exceed the built-in scratch limit of %d; "
+                            "use wt_forces with caller scratch",
+                            (long long)n_links, NOALLOC_MAX_BLOCKS * RED_THREADS);
+    if (!g || !g->f[0] || !g->f[1] || !out6) return wt_set_error(WT_ERR_ARG, "wt_forces_noalloc: null buffer");
+    if (n_links < 0 || (n_links > 0 && (!cells || !masks)))
+        return wt_set_error(WT_ERR_ARG, "wt_forces_noalloc: bad link list");
+    if (cur != 0 && cur != 1) return wt_set_error(WT_ERR_ARG, "wt_forces_noalloc: cur must be 0 or 1");
+    if (int rc = wt_check_dims(g->nx, g->ny, g->nz)) return rc;
+    double* partials = nullptr;
+    if (int rc = noalloc_scratch(&partials)) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (g->precision) {
+        case WT_F32: return forces_noalloc_impl<WT_F32>(g, cur, cells, masks, n_links, partials, out6, st);
+        case WT_F16: return forces_noalloc_impl<WT_F16>(g, cur, cells, masks, n_links, partials, out6, st);
+        case WT_BF16: return forces_noalloc_impl<WT_BF16>(g, cur, cells, masks, n_links, partials, out6, st);
+        case WT_F64: return forces_noalloc_impl<WT_F64>(g, cur, cells, masks, n_links, partials, out6, st);
+        default: return wt_set_error(WT_ERR_ARG, "wt_forces_noalloc: unknown precision %d", g->precision);
     }
 }

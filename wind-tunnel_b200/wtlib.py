@@ -15,12 +15,13 @@ WT_OK, WT_ERR_ARG, WT_ERR_DIMS, WT_ERR_CUDA, WT_ERR_CAPACITY, WT_ERR_TIMEOUT = 0
 F32, F16, BF16, F64 = 0, 1, 2, 3
 PRECISIONS = {'fp32': F32, 'fp16': F16, 'bf16': BF16, 'fp64': F64}
 STEP_MAC_ALL_LAST = 1
+NOALLOC_MAX_LINKS = 1048576  # wt_forces_noalloc limit (include/wt.h)
 COLLIDE_EXACT, COLLIDE_FAST = 0, 1
 
 # every symbol include/wt.h declares (tests check that the library exports them all)
 EXPORTS = ['wt_last_error', 'wt_abi_version', 'wt_check_dims', 'wt_population_bytes', 'wt_init_eq',
            'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step_tiles', 'wt_step',
-           'wt_reduce_scratch_len', 'wt_forces', 'wt_mass', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp']
+           'wt_reduce_scratch_len', 'wt_forces', 'wt_forces_noalloc', 'wt_mass', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp']
 
 
 class WtError(RuntimeError):
@@ -65,6 +66,7 @@ def lib():
             'wt_step': ([gp, i32, i32, f64, f64, f64, i32, vp], ctypes.c_int),
             'wt_reduce_scratch_len': ([i64], i64),
             'wt_forces': ([gp, i32, vp, vp, i64, vp, vp, vp], ctypes.c_int),
+            'wt_forces_noalloc': ([gp, i32, vp, vp, i64, vp, vp], ctypes.c_int),
             'wt_mass': ([gp, i32, vp, vp, vp], ctypes.c_int),
             'wt_advect': ([vp, vp, vp, vp, i32, i32, i32, i64, f32, f32, f32, u32, f32, f32, f32, f32, f32, vp],
                           ctypes.c_int),
