@@ -8,7 +8,7 @@
 //                   inlet cells; face cells whose interior neighbour has a LARGER linear
 //                   index read that neighbour's mac from the previous step (mac_prev); the
 //                   outlet cell x = nx-1 of an interior row takes the current values of its
-//                   x = nx-2 neighbour, which the same thread has just computed.
+//                   x = nx-2 neighbour from the same thread (V > 1) or the previous lane.
 //   k_step_faces -- the z = nz-1 plane and the y = ny-1 rows of interior z (x > 0): their
 //                   neighbour has a SMALLER linear index, so they read the mac that
 //                   k_step_bulk just wrote (mac_cur).
@@ -47,7 +47,7 @@ struct StepArgs {
     const uint8_t* solid;
     const uint8_t* code;
     int32_t nx, ny, nz, n, nxy;
-    FastDiv dnx, dny, dny2;
+    FastDiv dnx, dny;
     T uin, tau, csmag;  // csmag = 25.4558441 * smag * smag, evaluated in T left to right
     int32_t mac_all;
     // streaming kernel: 16-byte aligned copy bases (src[i] rounded down) and the remainders
@@ -474,36 +474,58 @@ __device__ __forceinline__ void store_cell(const StepArgs<typename P::S, typenam
 }
 
 // One cell outside the vector fast path: inlet, "previous-read" faces, solids and fluid
-// cells next to non-fluid cells. Cells that k_step_faces owns are skipped.
+// cells next to non-fluid cells. Cells of k_step_faces (z = nz-1 plane, y = ny-1 rows of
+// interior z) are skipped, and so is the outlet x = nx-1 of an interior row: the caller
+// handles it with outlet_cell once its x = nx-2 neighbour's values are known. The cell's
+// macro values (what it writes to mac) are returned in m*.
 template <class P, bool FAST>
 __device__ __forceinline__ void general_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx, int32_t x,
-                                             int32_t y, int32_t z, uint32_t code, bool face_row, bool row_shell) {
+                                             int32_t y, int32_t z, uint32_t code, bool face_row, bool row_shell,
+                                             typename P::T& mx, typename P::T& my, typename P::T& mz,
+                                             typename P::T& mr) {
     using T = typename P::T;
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
+    mx = (T)0.0; my = (T)0.0; mz = (T)0.0; mr = (T)1.0;
     const bool later = x > 0 && (face_row ? (z == nz - 1 || (y == ny - 1 && z > 0)) : x == nx - 1);
     if (later) return;
     bool write = a.mac_all;
-    T ox, oy, oz, orr;
     if (code & CODE_SOLID) {
-        ox = (T)0.0; oy = (T)0.0; oz = (T)0.0; orr = (T)1.0;
         write = write || (row_shell || (!face_row && (x == 1 || x == nx - 2)));
     } else if (x == 0) {
-        ox = a.uin; oy = (T)0.0; oz = (T)0.0; orr = (T)1.0;
+        mx = a.uin;
         face_eq<P>(a, idx, (T)1.0, a.uin, (T)0.0, (T)0.0);
     } else if (face_row) {
         const int32_t cxi = min(max(x, 1), nx - 2), cyi = min(max(y, 1), ny - 2), czi = min(max(z, 1), nz - 2);
         T px, py, pz, pr;
         load_mac(a.mac_prev, cxi + nx * (cyi + ny * czi), px, py, pz, pr);
-        face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, orr, ox, oy, oz);
-        face_eq<P>(a, idx, orr, ox, oy, oz);
+        face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, mr, mx, my, mz);
+        face_eq<P>(a, idx, mr, mx, my, mz);
     } else {
         T f[Q];
         pull_generic<P, FAST>(a, idx, (code & CODE_NEAR) != 0, f);
-        collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, ox, oy, oz, orr);
+        collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, mx, my, mz, mr);
         store_cell<P, FAST>(a, idx, f);
         write = write || row_shell || x == 1 || x == nx - 2;
     }
-    if (write) store_mac(a.mac_cur, idx, ox, oy, oz, orr);
+    if (write) store_mac(a.mac_cur, idx, mx, my, mz, mr);
+}
+
+// Outlet x = nx-1 of an interior row (server/lbm.py:101-103): equilibrium at rho = 1 from the
+// current values of its x = nx-2 neighbour (the neighbour has the smaller index, so in the
+// reference's serial order it is already updated).
+template <class P>
+__device__ __forceinline__ void outlet_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx, int32_t y,
+                                            int32_t z, uint32_t code, typename P::T qx, typename P::T qy,
+                                            typename P::T qz, typename P::T qr) {
+    using T = typename P::T;
+    if (code & CODE_SOLID) {
+        if (a.mac_all) store_mac(a.mac_cur, idx, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
+        return;
+    }
+    T br, bux, buy, buz;
+    face_values<T>(a.nx - 1, y, z, a.nx, a.ny, a.nz, a.uin, qx, qy, qz, qr, br, bux, buy, buz);
+    face_eq<P>(a, idx, br, bux, buy, buz);
+    if (a.mac_all) store_mac(a.mac_cur, idx, bux, buy, buz, br);
 }
 
 template <int PREC, bool FAST, int V, int BLOCK, int MINB>
@@ -513,21 +535,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_bulk(const StepArgs<typena
     using S = typename P::S;
     const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
     const int32_t idx0 = t * V;
-    if (idx0 >= a.n) return;
+    const bool valid = idx0 < a.n;
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t row = (int32_t)a.dnx.div((uint32_t)idx0);
-    const int32_t x0 = idx0 - row * nx;
+    const int32_t row = (int32_t)a.dnx.div((uint32_t)(valid ? idx0 : 0));
+    const int32_t x0 = (valid ? idx0 : 0) - row * nx;
     const int32_t z = (int32_t)a.dny.div((uint32_t)row);
     const int32_t y = row - z * ny;
     const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
     const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-
-    uint32_t codes;
-    if constexpr (V == 4) codes = *reinterpret_cast<const uint32_t*>(a.code + idx0);
-    else if constexpr (V == 2) codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
-    else codes = a.code[idx0];
-
-    if (!face_row && x0 > 0 && x0 + V <= nx - 1 && codes == 0) {
+    T mx = (T)0.0, my = (T)0.0, mz = (T)0.0, mr = (T)1.0;  // macro values of the latest cell
+    uint32_t codes = 0;
+    if (valid) {
+        if constexpr (V == 4) codes = *reinterpret_cast<const uint32_t*>(a.code + idx0);
+        else if constexpr (V == 2) codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
+        else codes = a.code[idx0];
+    }
+    if (valid && !face_row && x0 > 0 && x0 + V <= nx - 2 + (V == 1) && codes == 0) {
         // ---- fast path: V plain interior fluid cells, vector loads and stores ----
         T f[V][Q];
         unroll<0, Q>([&](auto ic) {
@@ -553,10 +576,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_bulk(const StepArgs<typena
         });
 #pragma unroll
         for (int k = 0; k < V; ++k) {
-            T ux, uy, uz, rho;
-            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, ux, uy, uz, rho);
-            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2)
-                store_mac(a.mac_cur, idx0 + k, ux, uy, uz, rho);
+            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, mx, my, mz, mr);
+            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2) store_mac(a.mac_cur, idx0 + k, mx, my, mz, mr);
         }
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
@@ -572,13 +593,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_bulk(const StepArgs<typena
                 vstore<S, V>(a.dst[i] + idx0, v);
             }
         });
-        return;
-    }
-
-    // ---- general path: cell by cell (faces, inlet, solids, cells next to solids) ----
+    } else if (valid) {
+        // ---- general path: cell by cell (faces, inlet, outlet, solids, cells next to solids) ----
 #pragma unroll 1
-    for (int k = 0; k < V; ++k)
-        general_cell<P, FAST>(a, idx0 + k, x0 + k, y, z, (codes >> (8 * k)) & 0xffu, face_row, row_shell);
+        for (int k = 0; k < V; ++k) {
+            const uint32_t code = (codes >> (8 * k)) & 0xffu;
+            if (V > 1 && !face_row && x0 + k == nx - 1) {
+                // its x = nx-2 neighbour is this thread's previous cell
+                outlet_cell<P>(a, idx0 + k, y, z, code, mx, my, mz, mr);
+            } else {
+                general_cell<P, FAST>(a, idx0 + k, x0 + k, y, z, code, face_row, row_shell, mx, my, mz, mr);
+            }
+        }
+    }
+    if constexpr (V == 1) {
+        // outlet with one cell per thread: nx is even, so the outlet index is odd and never
+        // starts a warp; its x = nx-2 neighbour is the previous lane
+        const T qx = __shfl_up_sync(0xffffffffu, mx, 1);
+        const T qy = __shfl_up_sync(0xffffffffu, my, 1);
+        const T qz = __shfl_up_sync(0xffffffffu, mz, 1);
+        const T qr = __shfl_up_sync(0xffffffffu, mr, 1);
+        if (valid && !face_row && x0 == nx - 1) outlet_cell<P>(a, idx0, y, z, codes, qx, qy, qz, qr);
+    }
 }
 
 template <int PREC>
@@ -588,24 +624,18 @@ __global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec
     const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
     const int32_t nplane = a.nxy, nrows = nx * (nz - 2);
-    if (t >= nplane + nrows + (ny - 2) * (nz - 2)) return;
+    if (t >= nplane + nrows) return;
     int32_t x, y, z;
     if (t < nplane) {  // z = nz-1 plane
         z = nz - 1;
         y = (int32_t)a.dnx.div((uint32_t)t);
         x = t - y * nx;
-    } else if (t < nplane + nrows) {  // y = ny-1 rows of interior z
+    } else {  // y = ny-1 rows of interior z
         const int32_t t2 = t - nplane;
         const int32_t r = (int32_t)a.dnx.div((uint32_t)t2);
         z = 1 + r;
         y = ny - 1;
         x = t2 - r * nx;
-    } else {  // outlet x = nx-1 of interior rows: its x = nx-2 neighbour was just updated
-        const int32_t t3 = t - nplane - nrows;
-        const int32_t r = (int32_t)a.dny2.div((uint32_t)t3);
-        z = 1 + r;
-        y = 1 + (t3 - r * (ny - 2));
-        x = nx - 1;
     }
     if (x == 0) return;
     const int32_t idx = x + nx * (y + ny * z);
@@ -829,6 +859,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
     // Consumer thread ct owns CPT consecutive cells of each chunk (L = 32 * CONSUMERS * CPT),
     // so a warp reads and writes contiguous runs; with CPT = 2 loads and stores are pairs.
     static_assert(L == 32 * CONSUMERS * CPT, "chunk = consumer threads x cells per thread");
+    static_assert(L % 32 == 0, "chunk starts at a warp boundary (outlet shuffle)");
     const int ct = threadIdx.x - 32;
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
 #pragma unroll 1
@@ -846,15 +877,19 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
         const int32_t c0 = k * L;
         const int32_t len = min(L, a.n - c0);
         const int32_t c = ct * CPT;
-        if (c < len) {  // len is a multiple of 16, so all CPT cells are in range
-            const int32_t idx = c0 + c;
+        const bool valid = c < len;  // len is a multiple of 16, so all CPT cells are in range
+        T mx = (T)0.0, my = (T)0.0, mz = (T)0.0, mr = (T)1.0;  // macro values of the latest cell
+        int32_t idx = 0, x = 0, y = 0, z = 0;
+        bool face_row = true;
+        uint32_t code = 0;
+        if (valid) {
+            idx = c0 + c;
             const int32_t row = (int32_t)a.dnx.div((uint32_t)idx);
-            const int32_t x = idx - row * nx;  // nx is a multiple of CPT: the cells share the row
-            const int32_t z = (int32_t)a.dny.div((uint32_t)row);
-            const int32_t y = row - z * ny;
-            const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+            x = idx - row * nx;  // nx is a multiple of CPT: the cells share the row
+            z = (int32_t)a.dny.div((uint32_t)row);
+            y = row - z * ny;
+            face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
             const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-            uint32_t code;
             if constexpr (CPT == 1) code = lds(codes + c);
             else code = lds(reinterpret_cast<const uint16_t*>(codes + c));
             if (!face_row && x > 0 && x + CPT < nx && code == 0) {
@@ -875,10 +910,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
                 });
 #pragma unroll
                 for (int q = 0; q < CPT; ++q) {
-                    T ux, uy, uz, rho;
-                    collide_any<P, FAST>(f[q], x + q, nx, a.tau, a.csmag, ux, uy, uz, rho);
+                    collide_any<P, FAST>(f[q], x + q, nx, a.tau, a.csmag, mx, my, mz, mr);
                     if (a.mac_all || row_shell || x + q == 1 || x + q == nx - 2)
-                        store_mac(a.mac_cur, idx + q, ux, uy, uz, rho);
+                        store_mac(a.mac_cur, idx + q, mx, my, mz, mr);
                 }
                 unroll<0, Q>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
@@ -896,9 +930,23 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
                 });
             } else {
 #pragma unroll 1
-                for (int q = 0; q < CPT; ++q)
-                    general_cell<P, FAST>(a, idx + q, x + q, y, z, (code >> (8 * q)) & 0xffu, face_row, row_shell);
+                for (int q = 0; q < CPT; ++q) {
+                    const uint32_t cq = (code >> (8 * q)) & 0xffu;
+                    if (CPT > 1 && !face_row && x + q == nx - 1)
+                        outlet_cell<P>(a, idx + q, y, z, cq, mx, my, mz, mr);  // neighbour: cell q-1
+                    else
+                        general_cell<P, FAST>(a, idx + q, x + q, y, z, cq, face_row, row_shell, mx, my, mz, mr);
+                }
             }
+        }
+        if constexpr (CPT == 1) {
+            // outlet: chunk starts are multiples of 32 and the outlet index is odd, so its
+            // x = nx-2 neighbour is the previous lane
+            const T qx = __shfl_up_sync(0xffffffffu, mx, 1);
+            const T qy = __shfl_up_sync(0xffffffffu, my, 1);
+            const T qz = __shfl_up_sync(0xffffffffu, mz, 1);
+            const T qr = __shfl_up_sync(0xffffffffu, mr, 1);
+            if (valid && !face_row && x == nx - 1) outlet_cell<P>(a, idx, y, z, code, qx, qy, qz, qr);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[st]);  // this warp is done with the stage
@@ -1006,7 +1054,6 @@ int step_impl(const wt_grid* g, int32_t cur, int32_t steps, double uin, double t
     a.n = a.nxy * g->nz;
     a.dnx = FastDiv((uint32_t)g->nx);
     a.dny = FastDiv((uint32_t)g->ny);
-    a.dny2 = FastDiv((uint32_t)(g->ny - 2));
     a.uin = (T)uin; a.tau = (T)tau;
     const T sm = (T)smag;
     a.csmag = (T)25.4558441 * sm * sm;  // same left-to-right product as server/lbm.py:152
@@ -1021,7 +1068,7 @@ int step_impl(const wt_grid* g, int32_t cur, int32_t steps, double uin, double t
     a.status = g->status;
     a.test_skip_chunk = g->test_skip_chunk;
     constexpr int VEC = 16 / (int)sizeof(S);
-    const int32_t nface = a.nxy + a.nx * (a.nz - 2) + (a.ny - 2) * (a.nz - 2);
+    const int32_t nface = a.nxy + a.nx * (a.nz - 2);
     const unsigned nb_face = (unsigned)((nface + 255) / 256);
     for (int32_t s = 0; s < steps; ++s) {
         const S* fin = static_cast<const S*>(g->f[cur]);
