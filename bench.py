@@ -267,13 +267,77 @@ def run_ours(args, rank, world, local_rank):
             del v
             torch.cuda.empty_cache()
 
+    batching = run_batching(dev) if args.batch and prec == 'fp32' else None
+
     acc = None
     if args.accuracy and prec == 'fp32' and rank == 0:
         import accuracy
         acc = accuracy.study(steps=args.accuracy_steps, scale=0.5, device=dev)
 
     return dict(value=value, t_dev=t_dev, roofline=roofline, e2e=e2e, clocks=clk.summary(), accuracy=acc,
+                batching=batching,
                 launches=launches_per_frame * args.steps, dims=dims, n=n, variants=variants)
+
+
+def run_batching(dev, replays=5, graph_steps=100):
+    """Config 4: 24 tunnels (0.5M-8M cells, 2:1:1, own obstacles and flow parameters) in one
+    batch: persistent bulk kernel over a tile work-list plus a face kernel per step, captured
+    as a CUDA graph of `graph_steps` steps. The batch tile is picked by timing each batched
+    tile shape. One tunnel is then re-run alone and compared bit for bit."""
+    import torch
+    import bodies
+    import lbm
+    from batch import TunnelBatch
+    cfg = bodies.config4()
+    solvers, params = [], []
+    for dims, solid, p in cfg:
+        s = lbm.Solver(dims, dev)
+        s.set_solid(solid)
+        s.reset(p['uIn'])
+        solvers.append(s)
+        params.append(p)
+    cells = sum(s.n for s in solvers)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tile_ms, steps_done = {}, 0
+    for tile in (1, 2, 3, 7):
+        b = TunnelBatch(solvers, params, tile=tile)
+        b.step(2)
+        ev0.record(b.stream)
+        b.step(4)
+        ev1.record(b.stream)
+        ev1.synchronize()
+        tile_ms[tile] = ev0.elapsed_time(ev1) / 4
+        steps_done += 6
+        b.close()
+    tile = min(tile_ms, key=tile_ms.get)
+    b = TunnelBatch(solvers, params, tile=tile)
+    b.capture(graph_steps)
+    b.replay()
+    steps_done += graph_steps
+    b.synchronize()
+    ev0.record(b.stream)
+    for _ in range(replays):
+        b.replay()
+    ev1.record(b.stream)
+    ev1.synchronize()
+    steps_done += replays * graph_steps
+    t = ev0.elapsed_time(ev1) / 1e3
+    b.close()
+    k = min(range(len(solvers)), key=lambda i: solvers[i].n)
+    dims, solid, p = cfg[k]
+    alone = lbm.Solver(dims, dev)
+    alone.set_solid(solid)
+    alone.reset(p['uIn'])
+    alone.step(steps_done, p)
+    same = bool(np.array_equal(alone.populations(), solvers[k].populations()))
+    out = {'tunnels': len(solvers), 'cells': cells, 'tile': tile,
+           'tile_ms_per_step': {str(a): round(v, 3) for a, v in tile_ms.items()},
+           'graph_steps': graph_steps, 'replays': replays, 'ms_per_step': round(t / (replays * graph_steps) * 1e3, 4),
+           'glups': round(cells * replays * graph_steps / t / 1e9, 3),
+           'checked_tunnel': list(dims), 'checked_steps': steps_done, 'bit_identical_to_alone': same}
+    del solvers, alone
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline(dims, solid, budget_s, threads=None):
@@ -315,6 +379,7 @@ def main():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-variants', dest='variants', action='store_false')
     ap.add_argument('--no-accuracy', dest='accuracy', action='store_false')
+    ap.add_argument('--no-batch', dest='batch', action='store_false')
     ap.add_argument('--accuracy-steps', type=int, default=2000)
     args = ap.parse_args()
 
@@ -356,6 +421,7 @@ def main():
                    'parallelism': f'replicas x{world}'},
         'roofline': r['roofline'], 'cpu_baseline': cpu, 'e2e': r['e2e'], 'clocks': r['clocks'],
         'gpu_launches': r['launches'], 'precision_variants': r['variants'], 'accuracy_vs_fp64': r['accuracy'],
+        'batching': r['batching'],
     }
     print(json.dumps(line), flush=True)
 

@@ -137,6 +137,29 @@ int wt_forces_noalloc(const wt_grid* g, int32_t cur, const int32_t* cells, const
 /* Total mass sum_{fluid cells} sum_i f_i of f[cur] in double, deterministic. */
 int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void* stream);
 
+/* ---- many tunnels at once ----
+ * A batch advances `count` tunnels of uneven sizes together: per step one persistent bulk
+ * kernel over a tile work-list spanning all tunnels, then one kernel over all tunnels' face
+ * cells. No counterpart in the reference, which runs one tunnel (server/app.py:116); each
+ * tunnel's results are bit-identical to stepping it alone with wt_step. All tunnels share
+ * precision and collision form; tile is a direct-load tile id of wt_step_tiles (0 =
+ * default). The caller allocates a 256-byte aligned device workspace of
+ * wt_batch_workspace_bytes (descriptor table and work lists). cur gives each tunnel's
+ * current population buffer at creation; wt_batch_cur reports it later. A batch must be
+ * re-created after any of its tunnels is stepped on its own. */
+typedef struct wt_batch wt_batch;
+int64_t wt_batch_workspace_bytes(const wt_grid* grids, int32_t count, int32_t tile);
+int wt_batch_create(const wt_grid* grids, int32_t count, const double* uin, const double* tau, const double* smag,
+                    const int32_t* cur, int32_t tile, void* workspace, int64_t workspace_bytes, void* stream,
+                    wt_batch** out);
+int wt_batch_step(wt_batch* b, int32_t steps, int32_t flags, void* stream);
+/* Capture `steps` (even) steps as a CUDA graph on a non-default stream; replay it with
+ * wt_batch_replay (each replay advances every tunnel by `steps` steps). */
+int wt_batch_capture(wt_batch* b, int32_t steps, int32_t flags, void* stream);
+int wt_batch_replay(wt_batch* b, void* stream);
+int wt_batch_cur(const wt_batch* b, int32_t* cur_out);
+int wt_batch_destroy(wt_batch* b);
+
 /* ---- frame outputs (Solver.frame, server/lbm.py:458-482) ---- */
 /* advect_kernel (server/lbm.py:233-263): RK2 streamline particles through mac.
  * Respawn uses this library's counter-based RNG (not Warp's). mac: float (4*n). */

@@ -1,0 +1,65 @@
+"""Many tunnels in one batch (wt_batch_*): each tunnel's populations must equal, bit for bit,
+the same tunnel stepped alone with wt_step, for direct steps, odd step counts and CUDA-graph
+replays."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _tunnels(collision='exact', precision='fp32'):
+    import bodies
+    from lbm import Solver
+    specs = [((64, 24, 20), 0.05, 0.51), ((48, 16, 16), 0.07, 0.53), ((96, 32, 24), 0.04, 0.505)]
+    out = []
+    for k, (dims, uin, tau) in enumerate(specs):
+        solid, _ = bodies.ellipsoid_union(dims, 2, 100 + k, scale=dims[0] / 256.0, floor='belt')
+        p = dict(uIn=uin, tau=tau, smag=0.16)
+        s = Solver(dims, 'cuda:0', precision=precision, collision=collision)
+        s.set_solid(solid)
+        s.reset(uin)
+        out.append((s, solid, p))
+    return out
+
+
+def _alone(dims, solid, p, steps, collision, precision):
+    from lbm import Solver
+    s = Solver(dims, 'cuda:0', precision=precision, collision=collision)
+    s.set_solid(solid)
+    s.reset(p['uIn'])
+    s.step(steps, p)
+    return s.populations(), s.macro()
+
+
+@pytest.mark.parametrize('collision,precision', [('exact', 'fp32'), ('fast', 'fp16')])
+@pytest.mark.parametrize('tile', [2, 3])
+def test_batch_equals_tunnels_alone(collision, precision, tile):
+    from batch import TunnelBatch
+    tun = _tunnels(collision, precision)
+    b = TunnelBatch([t[0] for t in tun], [t[2] for t in tun], tile=tile)
+    b.step(3)
+    b.step(4)
+    b.synchronize()
+    for s, solid, p in tun:
+        f, mac = _alone((s.nx, s.ny, s.nz), solid, p, 7, collision, precision)
+        assert s.cur == 1
+        assert np.array_equal(s.populations(), f)
+        assert np.array_equal(s.macro(), mac)
+    b.close()
+
+
+def test_batch_graph_replay_equals_steps():
+    from batch import TunnelBatch
+    tun = _tunnels()
+    b = TunnelBatch([t[0] for t in tun], [t[2] for t in tun], tile=2)
+    b.capture(10)
+    b.replay()
+    b.replay()
+    b.synchronize()
+    for s, solid, p in tun:
+        f, mac = _alone((s.nx, s.ny, s.nz), solid, p, 20, 'exact', 'fp32')
+        assert s.cur == 0
+        assert np.array_equal(s.populations(), f)
+        assert np.array_equal(s.macro(), mac)
+    b.close()

@@ -1,0 +1,79 @@
+"""Many tunnels advanced together (wt_batch_* of include/wt.h).
+
+``TunnelBatch`` groups Solvers of one device, precision and collision form. Each step runs
+one persistent bulk kernel over a tile work-list that spans every tunnel, then one kernel
+over all tunnels' face cells; ``capture(k)`` records k (even) steps as a CUDA graph that
+``replay()`` launches with a single call. Every tunnel's populations are bit-identical to
+stepping its Solver alone. After batch steps the Solvers' ``cur`` is kept in sync; a batch
+must be rebuilt after any member Solver is stepped on its own.
+"""
+import ctypes
+
+import torch
+
+import wtlib as W
+from wtlib import call, ptr
+
+
+class TunnelBatch:
+    def __init__(self, solvers, params, tile=0, stream=None):
+        if not solvers:
+            raise ValueError('empty batch')
+        self.solvers = list(solvers)
+        dev = self.solvers[0].dev
+        for s in self.solvers:
+            if s.dev != dev or s.precision != self.solvers[0].precision or s.collision != self.solvers[0].collision:
+                raise ValueError('a batch needs one device, precision and collision form')
+        self.dev = dev
+        self.stream = stream if stream is not None else torch.cuda.Stream(dev)
+        self.sh = W.stream_handle(self.stream)
+        n = len(self.solvers)
+        self.grids = (W.Grid * n)(*[s.grid for s in self.solvers])
+        dbl = ctypes.c_double * n
+        self._uin = dbl(*[float(p['uIn']) for p in params])
+        self._tau = dbl(*[float(p['tau']) for p in params])
+        self._smag = dbl(*[float(p['smag']) for p in params])
+        self._cur = (ctypes.c_int32 * n)(*[s.cur for s in self.solvers])
+        self.tile = int(tile)
+        nbytes = W.lib().wt_batch_workspace_bytes(self.grids, n, self.tile)
+        if nbytes < 0:
+            W.check(int(nbytes))
+        for s in self.solvers:  # the member tunnels' pending work comes first
+            self.stream.wait_stream(s.stream)
+        with torch.cuda.stream(self.stream):
+            self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+        self.handle = ctypes.c_void_p()
+        call('wt_batch_create', self.grids, n, self._uin, self._tau, self._smag, self._cur, self.tile,
+             ptr(self.workspace), int(nbytes), self.sh, ctypes.byref(self.handle))
+        self.cells = sum(s.n for s in self.solvers)
+
+    def _sync_cur(self):
+        cur = (ctypes.c_int32 * len(self.solvers))()
+        call('wt_batch_cur', self.handle, cur)
+        for s, c in zip(self.solvers, cur):
+            s.cur = int(c)
+
+    def step(self, steps, mac_all_last=True):
+        call('wt_batch_step', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
+        self._sync_cur()
+
+    def capture(self, steps, mac_all_last=True):
+        call('wt_batch_capture', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
+
+    def replay(self):
+        call('wt_batch_replay', self.handle, self.sh)
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+    def close(self):
+        if self.handle:
+            self.stream.synchronize()
+            W.lib().wt_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -148,3 +148,22 @@ def config2(scale=1.0, seed=2024):
     dims = (int(512 * scale), int(256 * scale), int(256 * scale))
     solid, _ = ellipsoid_union(dims, 6, seed, scale=scale, floor='belt')
     return dims, solid, dict(uIn=0.05, tau=3 * 0.001 + 0.5, smag=0.16)
+
+
+def config4(count=24, seed=4, cells=(0.5e6, 8e6)):
+    """Batching workload: `count` tunnels, cell counts log-uniform in `cells`, aspect 2:1:1
+    (nx = 2 ny = 2 nz, nx a multiple of 16), each with its own seeded union of 1-6 ellipsoids
+    on a moving belt, u0 uniform in [0.03, 0.08], nu uniform in [0.001, 0.01] (tau = 3 nu + 1/2).
+    Returns [(dims, solid, params)]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for t in range(count):
+        n = float(np.exp(rng.uniform(np.log(cells[0]), np.log(cells[1]))))
+        nx = max(32, int(round((4.0 * n) ** (1.0 / 3.0) / 16.0)) * 16)
+        dims = (nx, nx // 2, nx // 2)
+        k = int(rng.integers(1, 7))
+        solid, _ = ellipsoid_union(dims, k, int(rng.integers(1 << 31)), scale=nx / 512.0, floor='belt')
+        u0 = float(rng.uniform(0.03, 0.08))
+        nu = float(rng.uniform(0.001, 0.01))
+        out.append((dims, solid, dict(uIn=u0, tau=3.0 * nu + 0.5, smag=0.16)))
+    return out

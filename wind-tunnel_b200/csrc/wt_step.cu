@@ -1,957 +1,8 @@
-// Fused D3Q19 step: pull streaming + bounce-back / moving belt + equilibrium faces +
-// regularized collision with Smagorinsky eddy viscosity and outlet sponge.
-// Semantics: step_kernel of RICKxxROLLING/wind-tunnel server/lbm.py:72-166.
-//
-// One step = two launches:
-//   k_step_bulk  -- every cell except the "current-read" faces below. Each thread owns V
-//                   consecutive cells of one x-row. Interior cells pull and collide; x = 0
-//                   inlet cells; face cells whose interior neighbour has a LARGER linear
-//                   index read that neighbour's mac from the previous step (mac_prev); the
-//                   outlet cell x = nx-1 of an interior row takes the current values of its
-//                   x = nx-2 neighbour from the same thread (V > 1) or the previous lane.
-//   k_step_faces -- the z = nz-1 plane and the y = ny-1 rows of interior z (x > 0): their
-//                   neighbour has a SMALLER linear index, so they read the mac that
-//                   k_step_bulk just wrote (mac_cur).
-// That is exactly the value each face cell sees when the reference launch runs in tid
-// order (Warp's CPU backend), and it is deterministic, unlike the single-launch race of
-// server/lbm.py:87 vs :166 on a GPU.
-//
-// Memory: population i of the pull source of cell idx is src[i][idx] with
-// src[i] = fin + i*n - (c_ix + c_iy*nx + c_iz*nx*ny), so every load is one base pointer
-// (kernel parameter, uniform) plus idx. A thread whose V cells are all plain interior fluid
-// (the common case) loads each population with one aligned V-wide vector load, plus one
-// scalar for the ±x-shifted ones, and stores each output population with one vector store.
-//
-// mac is double-buffered: the step that writes f[b] writes mac[b]. Every step writes mac
-// for the shell of interior cells that faces read (coordinates 1 or n-2); with mac_all set
-// (the last step before a frame) every cell writes it, as the reference does.
-//
-// Arithmetic keeps the reference's association order (the library is built without FMA
-// contraction). Two rewrites are exact: a leading "0.0 +" of a generated sum is dropped
-// (it can only turn -0.0 into +0.0, which no later operation can observe here), and the
-// term 0.5*cu*cu is shared by opposite directions (cu of the opposite direction is the
-// exact negation).
-#include <algorithm>
-
-#include "wt_common.cuh"
+// Single-tunnel step entry point (wt_step) and the tile-variant table of the step kernels.
+// The kernels themselves are in wt_step_impl.cuh (shared with the batched form, wt_batch.cu).
+#include "wt_step_impl.cuh"
 
 namespace wt {
-
-template <class S, class T>
-struct StepArgs {
-    const S* src[Q];   // pull source bases, see above
-    S* dst[Q];         // fout + i*n
-    const S* fin;
-    const T* mac_prev;
-    T* mac_cur;
-    const uint8_t* solid;
-    const uint8_t* code;
-    int32_t nx, ny, nz, n, nxy;
-    FastDiv dnx, dny;
-    T uin, tau, csmag;  // csmag = 25.4558441 * smag * smag, evaluated in T left to right
-    int32_t mac_all;
-    // streaming kernel: 16-byte aligned copy bases (src[i] rounded down) and the remainders
-    const S* chunk_src[Q];
-    int32_t chunk_r[Q];
-    int32_t* status;           // device word for bounded-wait failures (may be null)
-    int32_t test_skip_chunk;   // test hook: when > 0, chunk test_skip_chunk-1 is never loaded
-};
-
-template <class T>
-__device__ __forceinline__ void store_mac(T* mac, int32_t idx, T a, T b, T c, T d) {
-    if constexpr (sizeof(T) == 4) {
-        reinterpret_cast<float4*>(mac)[idx] = make_float4(a, b, c, d);
-    } else {
-        reinterpret_cast<double2*>(mac)[2 * idx] = make_double2(a, b);
-        reinterpret_cast<double2*>(mac)[2 * idx + 1] = make_double2(c, d);
-    }
-}
-template <class T>
-__device__ __forceinline__ void load_mac(const T* mac, int32_t idx, T& a, T& b, T& c, T& d) {
-    if constexpr (sizeof(T) == 4) {
-        const float4 v = reinterpret_cast<const float4*>(mac)[idx];
-        a = v.x; b = v.y; c = v.z; d = v.w;
-    } else {
-        const double2 v0 = reinterpret_cast<const double2*>(mac)[2 * idx];
-        const double2 v1 = reinterpret_cast<const double2*>(mac)[2 * idx + 1];
-        a = v0.x; b = v0.y; c = v1.x; d = v1.y;
-    }
-}
-
-template <class T>
-__device__ __forceinline__ T clampv(T x, T lo, T hi) { return x < lo ? lo : (x > hi ? hi : x); }
-
-// aligned vector of V stored values
-template <class S, int V>
-struct SVec {
-    S v[V];
-};
-template <class S, int V>
-__device__ __forceinline__ SVec<S, V> vload(const S* p) {
-    SVec<S, V> r;
-    constexpr int B = (int)sizeof(S) * V;
-    static_assert(B == 4 || B == 8 || B == 16 || B == 32, "vector width");
-    if constexpr (B == 4) {
-        const uint32_t u = *reinterpret_cast<const uint32_t*>(p);
-        memcpy(&r, &u, 4);
-    } else if constexpr (B == 8) {
-        const uint2 u = *reinterpret_cast<const uint2*>(p);
-        memcpy(&r, &u, 8);
-    } else if constexpr (B == 16) {
-        const uint4 u = *reinterpret_cast<const uint4*>(p);
-        memcpy(&r, &u, 16);
-    } else {
-        const uint4 u0 = reinterpret_cast<const uint4*>(p)[0];
-        const uint4 u1 = reinterpret_cast<const uint4*>(p)[1];
-        memcpy(&r, &u0, 16);
-        memcpy(reinterpret_cast<char*>(&r) + 16, &u1, 16);
-    }
-    return r;
-}
-template <class S, int V>
-__device__ __forceinline__ void vstore(S* p, const SVec<S, V>& r) {
-    constexpr int B = (int)sizeof(S) * V;
-    if constexpr (B == 4) {
-        uint32_t u;
-        memcpy(&u, &r, 4);
-        *reinterpret_cast<uint32_t*>(p) = u;
-    } else if constexpr (B == 8) {
-        uint2 u;
-        memcpy(&u, &r, 8);
-        *reinterpret_cast<uint2*>(p) = u;
-    } else if constexpr (B == 16) {
-        uint4 u;
-        memcpy(&u, &r, 16);
-        *reinterpret_cast<uint4*>(p) = u;
-    } else {
-        uint4 u0, u1;
-        memcpy(&u0, &r, 16);
-        memcpy(&u1, reinterpret_cast<const char*>(&r) + 16, 16);
-        reinterpret_cast<uint4*>(p)[0] = u0;
-        reinterpret_cast<uint4*>(p)[1] = u1;
-    }
-}
-
-// Equilibrium face populations from (br, bux, buy, buz) (server/lbm.py:104-107).
-template <class P>
-__device__ __forceinline__ void face_eq(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
-                                        typename P::T br, typename P::T bux, typename P::T buy, typename P::T buz) {
-    using T = typename P::T;
-    const T bsq = (T)1.5 * (bux * bux + buy * buy + buz * buz);
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        T s = (T)0.0;
-        if constexpr (cx(i) > 0) s = s + bux;
-        if constexpr (cx(i) < 0) s = s - bux;
-        if constexpr (cy(i) > 0) s = s + buy;
-        if constexpr (cy(i) < 0) s = s - buy;
-        if constexpr (cz(i) > 0) s = s + buz;
-        if constexpr (cz(i) < 0) s = s - buz;
-        const T bc = (T)3.0 * s;
-        st_pop<P, i>(a.dst[i] + idx, (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq));
-    });
-}
-
-// Boundary values of a face cell from its clamped interior neighbour's mac
-// (server/lbm.py:87-103).
-template <class T>
-__device__ __forceinline__ void face_values(int32_t x, int32_t y, int32_t z, int32_t nx, int32_t ny, int32_t nz,
-                                            T uin, T mx, T my, T mz, T mr, T& br, T& bux, T& buy, T& buz) {
-    br = clampv(mr, (T)0.9, (T)1.1);
-    bux = mx; buy = my; buz = mz;
-    if (y == 0 || y == ny - 1) buy = (T)0.0;
-    if (z == 0 || z == nz - 1) buz = (T)0.0;
-    if (x == 0) {
-        br = (T)1.0; bux = uin; buy = (T)0.0; buz = (T)0.0;
-    } else if (x == nx - 1) {
-        br = (T)1.0; bux = bux < (T)0.0 ? (T)0.0 : bux;
-    }
-}
-
-// sum of c-signed terms in the generator's order with the leading "0.0 +" dropped
-template <int AX, class T>
-__device__ __forceinline__ T csum(const T (&f)[Q]) {
-    T acc = (T)0.0;
-    bool first = true;
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        constexpr int c = AX == 0 ? cx(i) : (AX == 1 ? cy(i) : cz(i));
-        if constexpr (c != 0) {
-            if (first) acc = c > 0 ? f[i] : -f[i];
-            else acc = c > 0 ? acc + f[i] : acc - f[i];
-            first = false;
-        }
-    });
-    return acc;
-}
-
-// Regularized Smagorinsky collision of one cell (server/lbm.py:125-166). f holds the
-// pulled populations on entry and the post-collision populations on exit.
-template <class T>
-__device__ __forceinline__ void collide(T (&f)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy, T& ouz,
-                                        T& orho) {
-    T rho = f[0];
-    unroll<1, Q>([&](auto ic) { rho = rho + f[decltype(ic)::value]; });
-    const T jx = csum<0>(f), jy = csum<1>(f), jz = csum<2>(f);
-    const T ir = (T)1.0 / rho;
-    T ux = jx * ir, uy = jy * ir, uz = jz * ir;
-    const T um = sqrt(ux * ux + uy * uy + uz * uz);
-    if (um > (T)0.35) {
-        const T sc = (T)0.35 / um;
-        ux = ux * sc; uy = uy * sc; uz = uz * sc;
-    }
-    const T usq = (T)1.5 * (ux * ux + uy * uy + uz * uz);
-    T e[Q];
-    // e_i = w rho (1 + cu + 0.5 cu cu - usq), d_i = f_i - e_i (f[] becomes d[])
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (i == 0) {
-            e[0] = (T)wd(0) * rho * ((T)1.0 - usq);
-            f[0] = f[0] - e[0];
-        } else if constexpr (opp(i) > i) {  // handle the pair (i, opp(i)) together
-            constexpr int o = opp(i);
-            T s;
-            bool first = true;
-            if constexpr (cx(i) != 0) { s = cx(i) > 0 ? ux : -ux; first = false; }
-            if constexpr (cy(i) != 0) {
-                if (first) s = cy(i) > 0 ? uy : -uy;
-                else s = cy(i) > 0 ? s + uy : s - uy;
-                first = false;
-            }
-            if constexpr (cz(i) != 0) {
-                if (first) s = cz(i) > 0 ? uz : -uz;
-                else s = cz(i) > 0 ? s + uz : s - uz;
-            }
-            const T cu = (T)3.0 * s;
-            const T q = (T)0.5 * cu * cu;
-            const T wr = (T)wd(i) * rho;
-            e[i] = wr * ((T)1.0 + cu + q - usq);
-            e[o] = wr * ((T)1.0 - cu + q - usq);
-            f[i] = f[i] - e[i];
-            f[o] = f[o] - e[o];
-        }
-    });
-    T pxx, pyy, pzz, pxy, pxz, pyz;
-    {
-        bool fx = true, fy = true, fz = true, fxy = true, fxz = true, fyz = true;
-        pxx = pyy = pzz = pxy = pxz = pyz = (T)0.0;
-        unroll<0, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            if constexpr (cx(i) != 0) { pxx = fx ? f[i] : pxx + f[i]; fx = false; }
-            if constexpr (cy(i) != 0) { pyy = fy ? f[i] : pyy + f[i]; fy = false; }
-            if constexpr (cz(i) != 0) { pzz = fz ? f[i] : pzz + f[i]; fz = false; }
-            if constexpr (cx(i) * cy(i) != 0) {
-                pxy = fxy ? (cx(i) * cy(i) > 0 ? f[i] : -f[i]) : (cx(i) * cy(i) > 0 ? pxy + f[i] : pxy - f[i]);
-                fxy = false;
-            }
-            if constexpr (cx(i) * cz(i) != 0) {
-                pxz = fxz ? (cx(i) * cz(i) > 0 ? f[i] : -f[i]) : (cx(i) * cz(i) > 0 ? pxz + f[i] : pxz - f[i]);
-                fxz = false;
-            }
-            if constexpr (cy(i) * cz(i) != 0) {
-                pyz = fyz ? (cy(i) * cz(i) > 0 ? f[i] : -f[i]) : (cy(i) * cz(i) > 0 ? pyz + f[i] : pyz - f[i]);
-                fyz = false;
-            }
-        });
-    }
-    const T qn = sqrt(pxx * pxx + pyy * pyy + pzz * pzz + (T)2.0 * (pxy * pxy + pxz * pxz + pyz * pyz));
-    T tau0 = tau;
-    const T sp = (T)x - (T)nx + (T)24.0;
-    if (sp > (T)0.0) tau0 = tau0 + sp * (T)0.015;
-    const T tau_e = (T)0.5 * (tau0 + sqrt(tau0 * tau0 + csmag * qn * ir));
-    const T keep = (T)1.0 - (T)1.0 / tau_e;
-    const T tr3 = (pxx + pyy + pzz) * ((T)1.0 / (T)3.0);
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        // the generator's ' + '.join(terms) + ' - tr3' (server/lbm.py:157-164)
-        T qp;
-        if constexpr (i == 0) {
-            qp = -tr3;
-        } else {
-            constexpr bool hx = cx(i) != 0, hy = cy(i) != 0, hz = cz(i) != 0;
-            T acc = hx ? pxx : (hy ? pyy : pzz);
-            if constexpr (hx && hy) acc = acc + pyy;
-            if constexpr ((hx || hy) && hz) acc = acc + pzz;
-            if constexpr (hx && hy) acc = acc + (T)(2 * cx(i) * cy(i)) * pxy;
-            if constexpr (hx && hz) acc = acc + (T)(2 * cx(i) * cz(i)) * pxz;
-            if constexpr (hy && hz) acc = acc + (T)(2 * cy(i) * cz(i)) * pyz;
-            qp = acc - tr3;
-        }
-        f[i] = e[i] + (T)(4.5 * wd(i)) * keep * qp;
-    });
-    oux = ux; ouy = uy; ouz = uz; orho = rho;
-}
-
-// fused multiply-add, rounded once (explicit: the library is built without contraction)
-__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
-
-// Moment-space form of the same regularized Smagorinsky collision (mathematically equal
-// to collide(): on D3Q19 the second moment of the second-order equilibrium is
-// rho (u u + I/3), so Pi_neq = sum_i f_i c_i c_i - rho (u u + I/3), and every output is
-// w_i (B + 3 rho c.u + 4.5 rho (c.u)^2 + c c : A) with A = 4.5 (1 - 1/tau_e) Pi_neq and
-// B = rho (1 - 1.5 u.u) - tr(A)/3). Opposite directions share all but the sign of the odd
-// term. About 200 floating-point operations per cell against 330 in the reference order.
-// With SHIFT the inputs and outputs are deviations v_i = f_i - w_i (the fp16/bf16 storage
-// form): the constant parts cancel analytically, which keeps small numbers small.
-// Reciprocals and square roots use the special-function unit (rcp_fast etc.), so results
-// match the oracle's IEEE restatement of this form to within a few float ulps.
-// Reciprocal and square roots for the fast form: the special-function unit's
-// approximation refined by one Newton step (about 1 ulp in float); IEEE ops in double.
-__device__ __forceinline__ float rcp_fast(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    const float e = __fmaf_rn(-x, r, 1.0f);
-    return __fmaf_rn(r, e, r);
-}
-__device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
-__device__ __forceinline__ float sqrt_fast(float x) {  // x >= 0 (0 maps to 0)
-    float r;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-__device__ __forceinline__ double sqrt_fast(double x) { return sqrt(x); }
-__device__ __forceinline__ float rsqrt_fast(float x) {  // x > 0
-    float r;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    const float h = __fmul_rn(__fmul_rn(0.5f, x), __fmul_rn(r, r));
-    return __fmul_rn(r, __fsub_rn(1.5f, h));
-}
-__device__ __forceinline__ double rsqrt_fast(double x) { return 1.0 / sqrt(x); }
-
-template <class T, bool SHIFT>
-__device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy,
-                                             T& ouz, T& orho) {
-    const T s1 = v[1] + v[2], a1 = v[1] - v[2];
-    const T s3 = v[3] + v[4], a3 = v[3] - v[4];
-    const T s5 = v[5] + v[6], a5 = v[5] - v[6];
-    const T s7 = v[7] + v[8], a7 = v[7] - v[8];
-    const T s9 = v[9] + v[10], a9 = v[9] - v[10];
-    const T s11 = v[11] + v[12], a11 = v[11] - v[12];
-    const T s13 = v[13] + v[14], a13 = v[13] - v[14];
-    const T s15 = v[15] + v[16], a15 = v[15] - v[16];
-    const T s17 = v[17] + v[18], a17 = v[17] - v[18];
-    const T d7 = s7 + s9, d11 = s11 + s13, d15 = s15 + s17;
-    const T xxx = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
-    const T xxy = s7 - s9, xxz = s11 - s13, xyz = s15 - s17;
-    const T S = ((v[0] + s1) + (s3 + s5)) + ((d7 + d11) + d15);
-    const T jx = ((a1 + a7) + (a9 + a11)) + a13;
-    const T jy = ((a3 + a7) - (a9 - a15)) + a17;
-    const T jz = ((a5 + a11) - (a13 - a15)) - a17;
-    const T rho = SHIFT ? S + (T)1.0 : S;
-    const T ir = rcp_fast(rho);
-    T ux = jx * ir, uy = jy * ir, uz = jz * ir;
-    T usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
-    if (usq > (T)0.1225) {  // |u| > 0.35 (server/lbm.py:131-135)
-        const T sc = (T)0.35 * rsqrt_fast(usq);
-        ux = ux * sc; uy = uy * sc; uz = uz * sc;
-        usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
-    }
-    const T rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
-    const T t3 = (SHIFT ? S : rho) * ((T)1.0 / (T)3.0);
-    const T nxx = fmaT(-rux, ux, xxx - t3), nyy = fmaT(-ruy, uy, xyy - t3), nzz = fmaT(-ruz, uz, xzz - t3);
-    const T nxy = fmaT(-rux, uy, xxy), nxz = fmaT(-rux, uz, xxz), nyz = fmaT(-ruy, uz, xyz);
-    const T q1 = fmaT(nzz, nzz, fmaT(nyy, nyy, nxx * nxx));
-    const T q2 = fmaT(nyz, nyz, fmaT(nxz, nxz, nxy * nxy));
-    const T qn = sqrt_fast(fmaT((T)2.0, q2, q1));
-    T tau0 = tau;
-    const T sp = (T)x - (T)(nx - 24);  // outlet sponge (server/lbm.py:149-151)
-    if (sp > (T)0.0) tau0 = fmaT(sp, (T)0.015, tau);
-    const T tau_e = (T)0.5 * (tau0 + sqrt_fast(fmaT(tau0, tau0, csmag * qn * ir)));
-    const T keep = (T)1.0 - rcp_fast(tau_e);
-    const T k45 = (T)4.5 * keep, k9 = (T)9.0 * keep;
-    const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
-    const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;  // 2 A_ab
-    const T tra3 = ((axx + ayy) + azz) * ((T)1.0 / (T)3.0);
-    const T B = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
-    const T w0 = (T)wd(0), w1 = (T)wd(1), w2 = (T)wd(7);
-    const T w1x3 = (T)(3.0 * wd(1)), w2x3 = (T)(3.0 * wd(7));
-    v[0] = w0 * B;
-    const T bxx = B + axx, byy = B + ayy;
-    {
-        const T D = fmaT((T)4.5 * rux, ux, bxx), E = w1x3 * rux;
-        v[1] = fmaT(w1, D, E); v[2] = fmaT(w1, D, -E);
-    }
-    {
-        const T D = fmaT((T)4.5 * ruy, uy, byy), E = w1x3 * ruy;
-        v[3] = fmaT(w1, D, E); v[4] = fmaT(w1, D, -E);
-    }
-    {
-        const T D = fmaT((T)4.5 * ruz, uz, B + azz), E = w1x3 * ruz;
-        v[5] = fmaT(w1, D, E); v[6] = fmaT(w1, D, -E);
-    }
-    const T pxy = bxx + ayy, pxz = bxx + azz, pyz = byy + azz;
-    {
-        const T su = ux + uy, rs = rux + ruy;
-        const T D = fmaT((T)4.5 * rs, su, pxy + axy), E = w2x3 * rs;
-        v[7] = fmaT(w2, D, E); v[8] = fmaT(w2, D, -E);
-    }
-    {
-        const T su = ux - uy, rs = rux - ruy;
-        const T D = fmaT((T)4.5 * rs, su, pxy - axy), E = w2x3 * rs;
-        v[9] = fmaT(w2, D, E); v[10] = fmaT(w2, D, -E);
-    }
-    {
-        const T su = ux + uz, rs = rux + ruz;
-        const T D = fmaT((T)4.5 * rs, su, pxz + axz), E = w2x3 * rs;
-        v[11] = fmaT(w2, D, E); v[12] = fmaT(w2, D, -E);
-    }
-    {
-        const T su = ux - uz, rs = rux - ruz;
-        const T D = fmaT((T)4.5 * rs, su, pxz - axz), E = w2x3 * rs;
-        v[13] = fmaT(w2, D, E); v[14] = fmaT(w2, D, -E);
-    }
-    {
-        const T su = uy + uz, rs = ruy + ruz;
-        const T D = fmaT((T)4.5 * rs, su, pyz + ayz), E = w2x3 * rs;
-        v[15] = fmaT(w2, D, E); v[16] = fmaT(w2, D, -E);
-    }
-    {
-        const T su = uy - uz, rs = ruy - ruz;
-        const T D = fmaT((T)4.5 * rs, su, pyz - ayz), E = w2x3 * rs;
-        v[17] = fmaT(w2, D, E); v[18] = fmaT(w2, D, -E);
-    }
-    oux = ux; ouy = uy; ouz = uz; orho = rho;
-}
-
-// collision dispatch: FAST selects the moment-space form, on deviations for shifted storage
-template <class P, bool FAST>
-__device__ __forceinline__ void collide_any(typename P::T (&f)[Q], int32_t x, int32_t nx, typename P::T tau,
-                                            typename P::T csmag, typename P::T& ux, typename P::T& uy,
-                                            typename P::T& uz, typename P::T& rho) {
-    if constexpr (FAST) collide_fast<typename P::T, P::shifted>(f, x, nx, tau, csmag, ux, uy, uz, rho);
-    else collide<typename P::T>(f, x, nx, tau, csmag, ux, uy, uz, rho);
-}
-
-// population value as the collision of mode FAST takes it: f_i (+ w_i undone for shifted
-// storage in the exact form), or the stored deviation itself in the fast form
-template <class P, bool FAST, int I>
-__device__ __forceinline__ typename P::T ld_in(const typename P::S* p) {
-    if constexpr (FAST) return P::to(*p);
-    else return ld_pop<P, I>(p);
-}
-
-template <class P, bool FAST, int I>
-__device__ __forceinline__ void st_out(typename P::S* p, typename P::T v) {
-    if constexpr (FAST) *p = P::from(v);
-    else st_pop<P, I>(p, v);
-}
-
-// Pull of one cell with bounce-back and moving belt where a source is non-fluid
-// (server/lbm.py:110-124).
-template <class P, bool FAST>
-__device__ __forceinline__ void pull_generic(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
-                                             bool near, typename P::T (&f)[Q]) {
-    using T = typename P::T;
-    f[0] = ld_in<P, FAST, 0>(a.src[0] + idx);
-    unroll<1, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if (!near) {
-            f[i] = ld_in<P, FAST, i>(a.src[i] + idx);
-        } else {
-            const int32_t off = cx(i) + cy(i) * a.nx + cz(i) * a.nxy;
-            const int t = a.solid[idx - off];
-            if (t == 0) {
-                f[i] = ld_in<P, FAST, i>(a.src[i] + idx);
-            } else {
-                // bounce-back; in deviation form w_opp(i) = w_i, so the value carries over
-                f[i] = ld_in<P, FAST, opp(i)>(a.fin + (int64_t)opp(i) * a.n + idx);
-                if constexpr (cx(i) != 0) {
-                    if (t == 2) f[i] = f[i] + (T)(6.0 * wd(i) * cx(i)) * a.uin;
-                }
-            }
-        }
-    });
-}
-
-template <class P, bool FAST>
-__device__ __forceinline__ void store_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
-                                           const typename P::T (&f)[Q]) {
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        st_out<P, FAST, i>(a.dst[i] + idx, f[i]);
-    });
-}
-
-// One cell outside the vector fast path: inlet, "previous-read" faces, solids and fluid
-// cells next to non-fluid cells. Cells of k_step_faces (z = nz-1 plane, y = ny-1 rows of
-// interior z) are skipped, and so is the outlet x = nx-1 of an interior row: the caller
-// handles it with outlet_cell once its x = nx-2 neighbour's values are known. The cell's
-// macro values (what it writes to mac) are returned in m*.
-template <class P, bool FAST>
-__device__ __forceinline__ void general_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx, int32_t x,
-                                             int32_t y, int32_t z, uint32_t code, bool face_row, bool row_shell,
-                                             typename P::T& mx, typename P::T& my, typename P::T& mz,
-                                             typename P::T& mr) {
-    using T = typename P::T;
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    mx = (T)0.0; my = (T)0.0; mz = (T)0.0; mr = (T)1.0;
-    const bool later = x > 0 && (face_row ? (z == nz - 1 || (y == ny - 1 && z > 0)) : x == nx - 1);
-    if (later) return;
-    bool write = a.mac_all;
-    if (code & CODE_SOLID) {
-        write = write || (row_shell || (!face_row && (x == 1 || x == nx - 2)));
-    } else if (x == 0) {
-        mx = a.uin;
-        face_eq<P>(a, idx, (T)1.0, a.uin, (T)0.0, (T)0.0);
-    } else if (face_row) {
-        const int32_t cxi = min(max(x, 1), nx - 2), cyi = min(max(y, 1), ny - 2), czi = min(max(z, 1), nz - 2);
-        T px, py, pz, pr;
-        load_mac(a.mac_prev, cxi + nx * (cyi + ny * czi), px, py, pz, pr);
-        face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, mr, mx, my, mz);
-        face_eq<P>(a, idx, mr, mx, my, mz);
-    } else {
-        T f[Q];
-        pull_generic<P, FAST>(a, idx, (code & CODE_NEAR) != 0, f);
-        collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, mx, my, mz, mr);
-        store_cell<P, FAST>(a, idx, f);
-        write = write || row_shell || x == 1 || x == nx - 2;
-    }
-    if (write) store_mac(a.mac_cur, idx, mx, my, mz, mr);
-}
-
-// Outlet x = nx-1 of an interior row (server/lbm.py:101-103): equilibrium at rho = 1 from the
-// current values of its x = nx-2 neighbour (the neighbour has the smaller index, so in the
-// reference's serial order it is already updated).
-template <class P>
-__device__ __forceinline__ void outlet_cell(const StepArgs<typename P::S, typename P::T>& a, int32_t idx, int32_t y,
-                                            int32_t z, uint32_t code, typename P::T qx, typename P::T qy,
-                                            typename P::T qz, typename P::T qr) {
-    using T = typename P::T;
-    if (code & CODE_SOLID) {
-        if (a.mac_all) store_mac(a.mac_cur, idx, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
-        return;
-    }
-    T br, bux, buy, buz;
-    face_values<T>(a.nx - 1, y, z, a.nx, a.ny, a.nz, a.uin, qx, qy, qz, qr, br, bux, buy, buz);
-    face_eq<P>(a, idx, br, bux, buy, buz);
-    if (a.mac_all) store_mac(a.mac_cur, idx, bux, buy, buz, br);
-}
-
-template <int PREC, bool FAST, int V, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_step_bulk(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
-    using P = Prec<PREC>;
-    using T = typename P::T;
-    using S = typename P::S;
-    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int32_t idx0 = t * V;
-    const bool valid = idx0 < a.n;
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t row = (int32_t)a.dnx.div((uint32_t)(valid ? idx0 : 0));
-    const int32_t x0 = (valid ? idx0 : 0) - row * nx;
-    const int32_t z = (int32_t)a.dny.div((uint32_t)row);
-    const int32_t y = row - z * ny;
-    const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
-    const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-    T mx = (T)0.0, my = (T)0.0, mz = (T)0.0, mr = (T)1.0;  // macro values of the latest cell
-    uint32_t codes = 0;
-    if (valid) {
-        if constexpr (V == 4) codes = *reinterpret_cast<const uint32_t*>(a.code + idx0);
-        else if constexpr (V == 2) codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
-        else codes = a.code[idx0];
-    }
-    if (valid && !face_row && x0 > 0 && x0 + V <= nx - 2 + (V == 1) && codes == 0) {
-        // ---- fast path: V plain interior fluid cells, vector loads and stores ----
-        T f[V][Q];
-        unroll<0, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            const S* p = a.src[i] + idx0;
-            if constexpr (V == 1) {
-                f[0][i] = ld_in<P, FAST, i>(p);
-            } else {
-                const SVec<S, V> v = vload<S, V>(p + cx(i));  // aligned: the shift cancels
-                if constexpr (cx(i) == 0) {
-#pragma unroll
-                    for (int k = 0; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k]);
-                } else if constexpr (cx(i) > 0) {
-                    f[0][i] = ld_in<P, FAST, i>(p);
-#pragma unroll
-                    for (int k = 1; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k - 1]);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < V - 1; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k + 1]);
-                    f[V - 1][i] = ld_in<P, FAST, i>(p + V - 1);
-                }
-            }
-        });
-#pragma unroll
-        for (int k = 0; k < V; ++k) {
-            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, mx, my, mz, mr);
-            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2) store_mac(a.mac_cur, idx0 + k, mx, my, mz, mr);
-        }
-        unroll<0, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            if constexpr (V == 1) {
-                st_out<P, FAST, i>(a.dst[i] + idx0, f[0][i]);
-            } else {
-                SVec<S, V> v;
-#pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    if constexpr (P::shifted && !FAST) v.v[k] = P::from(f[k][i] - (T)wd(i));
-                    else v.v[k] = P::from(f[k][i]);
-                }
-                vstore<S, V>(a.dst[i] + idx0, v);
-            }
-        });
-    } else if (valid) {
-        // ---- general path: cell by cell (faces, inlet, outlet, solids, cells next to solids) ----
-#pragma unroll 1
-        for (int k = 0; k < V; ++k) {
-            const uint32_t code = (codes >> (8 * k)) & 0xffu;
-            if (V > 1 && !face_row && x0 + k == nx - 1) {
-                // its x = nx-2 neighbour is this thread's previous cell
-                outlet_cell<P>(a, idx0 + k, y, z, code, mx, my, mz, mr);
-            } else {
-                general_cell<P, FAST>(a, idx0 + k, x0 + k, y, z, code, face_row, row_shell, mx, my, mz, mr);
-            }
-        }
-    }
-    if constexpr (V == 1) {
-        // outlet with one cell per thread: nx is even, so the outlet index is odd and never
-        // starts a warp; its x = nx-2 neighbour is the previous lane
-        const T qx = __shfl_up_sync(0xffffffffu, mx, 1);
-        const T qy = __shfl_up_sync(0xffffffffu, my, 1);
-        const T qz = __shfl_up_sync(0xffffffffu, mz, 1);
-        const T qr = __shfl_up_sync(0xffffffffu, mr, 1);
-        if (valid && !face_row && x0 == nx - 1) outlet_cell<P>(a, idx0, y, z, codes, qx, qy, qz, qr);
-    }
-}
-
-template <int PREC>
-__global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
-    using P = Prec<PREC>;
-    using T = typename P::T;
-    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t nplane = a.nxy, nrows = nx * (nz - 2);
-    if (t >= nplane + nrows) return;
-    int32_t x, y, z;
-    if (t < nplane) {  // z = nz-1 plane
-        z = nz - 1;
-        y = (int32_t)a.dnx.div((uint32_t)t);
-        x = t - y * nx;
-    } else {  // y = ny-1 rows of interior z
-        const int32_t t2 = t - nplane;
-        const int32_t r = (int32_t)a.dnx.div((uint32_t)t2);
-        z = 1 + r;
-        y = ny - 1;
-        x = t2 - r * nx;
-    }
-    if (x == 0) return;
-    const int32_t idx = x + nx * (y + ny * z);
-    if (a.code[idx] & CODE_SOLID) {
-        if (a.mac_all) store_mac(a.mac_cur, idx, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
-        return;
-    }
-    const int32_t cxi = min(max(x, 1), nx - 2), cyi = min(max(y, 1), ny - 2), czi = min(max(z, 1), nz - 2);
-    T px, py, pz, pr, br, bux, buy, buz;
-    load_mac(a.mac_cur, cxi + nx * (cyi + ny * czi), px, py, pz, pr);
-    face_values<T>(x, y, z, nx, ny, nz, a.uin, px, py, pz, pr, br, bux, buy, buz);
-    face_eq<P>(a, idx, br, bux, buy, buz);
-    if (a.mac_all) store_mac(a.mac_cur, idx, bux, buy, buz, br);
-}
-
-// ---------------------------------------------------------------------------------
-// Streaming form of the bulk kernel: shared-memory staging through bulk async copies.
-//
-// With pull streaming, the destination cells [c0, c0 + L) read population i from the
-// contiguous source range src[i][c0 .. c0 + L): every population of a chunk of cells is
-// one 1-D bulk copy (cp.async.bulk, no tensor map, no multicast). The copy starts at the
-// 16-byte boundary at or below the range (chunk_src[i] = src[i] - chunk_r[i]) and is one
-// vector longer, so the cell at chunk offset c is stage[i][chunk_r[i] + c].
-//
-// Warp-specialised pipeline of NS stages per CTA: warp 0 is the producer (one lane issues
-// the 19 population copies and the chunk's code bytes into a free stage and arms the
-// stage's "full" mbarrier with the byte count); the other warps consume (wait on "full",
-// update their cells from shared memory, store to global memory, then arrive on the
-// stage's "empty" mbarrier). There is no CTA-wide barrier in the loop, so a consumer warp
-// slowed by boundary cells does not hold the others back. Persistent CTAs walk chunks
-// blockIdx.x + j*gridDim.x. Every wait is bounded; a wait that gives up sets the tunnel's
-// status word to WT_ERR_TIMEOUT and the warp leaves.
-// ---------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-// try_wait suspends the thread until the phase completes or ~SUSPEND_NS elapse
-constexpr uint32_t SUSPEND_NS = 1000;
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "n"(SUSPEND_NS)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: gives up after WAIT_LIMIT tries, about a second.
-constexpr uint32_t WAIT_LIMIT = 1u << 20;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
-template <class S>
-__device__ __forceinline__ S lds(const S* p) {
-    static_assert(sizeof(S) == 1 || sizeof(S) == 2 || sizeof(S) == 4 || sizeof(S) == 8, "lds width");
-    const uint32_t a = smem_u32(p);
-    if constexpr (sizeof(S) == 1) {
-        unsigned short v;
-        asm volatile("ld.shared.u8 %0, [%1];" : "=h"(v) : "r"(a));
-        return (S)v;
-    } else if constexpr (sizeof(S) == 4) {
-        float v;
-        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
-        return *reinterpret_cast<S*>(&v);
-    } else if constexpr (sizeof(S) == 2) {
-        unsigned short v;
-        asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
-        return *reinterpret_cast<S*>(&v);
-    } else {
-        double v;
-        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
-        return *reinterpret_cast<S*>(&v);
-    }
-}
-template <class S>
-__device__ __forceinline__ void sts(S* p, S v) {
-    static_assert(sizeof(S) == 2 || sizeof(S) == 4 || sizeof(S) == 8, "sts width");
-    const uint32_t a = smem_u32(p);
-    if constexpr (sizeof(S) == 4) {
-        asm volatile("st.shared.b32 [%0], %1;" ::"r"(a), "r"(*reinterpret_cast<uint32_t*>(&v)) : "memory");
-    } else if constexpr (sizeof(S) == 2) {
-        asm volatile("st.shared.b16 [%0], %1;" ::"r"(a), "h"(*reinterpret_cast<unsigned short*>(&v)) : "memory");
-    } else {
-        asm volatile("st.shared.b64 [%0], %1;" ::"r"(a), "l"(*reinterpret_cast<unsigned long long*>(&v)) : "memory");
-    }
-}
-
-template <class S>
-__device__ __forceinline__ SVec<S, 2> lds_pair(const S* p) {  // p aligned to 2 elements
-    SVec<S, 2> r;
-    const uint32_t a = smem_u32(p);
-    if constexpr (sizeof(S) == 2) {
-        uint32_t v;
-        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
-        memcpy(&r, &v, 4);
-    } else if constexpr (sizeof(S) == 4) {
-        uint2 v;
-        asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
-        memcpy(&r, &v, 8);
-    } else {
-        uint4 v;
-        asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
-        memcpy(&r, &v, 16);
-    }
-    return r;
-}
-// the same from a shared-memory stage
-template <class P, bool FAST, int I>
-__device__ __forceinline__ typename P::T ld_in_smem(const typename P::S* p) {
-    const typename P::S v = lds(p);
-    return ld_in<P, FAST, I>(&v);
-}
-
-template <class S, int L>
-struct StreamLayout {
-    static constexpr int VEC = 16 / (int)sizeof(S);
-    static constexpr int LP = L + VEC;                        // elements per population buffer
-    static constexpr int POP_BYTES = LP * (int)sizeof(S);     // multiple of 16
-    static constexpr int STAGE_BYTES = Q * POP_BYTES + L;     // populations + code bytes
-    static_assert(L % 16 == 0, "chunk length");
-};
-
-template <int PREC, int L>
-__device__ __forceinline__ bool stream_issue(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
-                                             unsigned char* stage, uint64_t* full, int32_t chunk) {
-    using S = typename Prec<PREC>::S;
-    using LY = StreamLayout<S, L>;
-    if (chunk + 1 == a.test_skip_chunk) return false;  // test hook: leave the stage empty
-    const int32_t c0 = chunk * L;
-    const int32_t len = min(L, a.n - c0);
-    const int32_t len16 = (len + LY::VEC - 1) / LY::VEC * LY::VEC;
-    const uint32_t pop_bytes = (uint32_t)((len16 + LY::VEC) * (int)sizeof(S));
-    const uint32_t code_bytes = (uint32_t)((len + 15) / 16 * 16);
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(full, Q * pop_bytes + code_bytes);
-#pragma unroll 1
-    for (int i = 0; i < Q; ++i) bulk_g2s(stage + i * LY::POP_BYTES, a.chunk_src[i] + c0, pop_bytes, full);
-    bulk_g2s(stage + Q * LY::POP_BYTES, a.code + c0, code_bytes, full);
-    return true;
-}
-
-template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB, int CPT>
-__global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
-    using P = Prec<PREC>;
-    using T = typename P::T;
-    using S = typename P::S;
-    using LY = StreamLayout<S, L>;
-    constexpr int CONSUMERS = THREADS / 32 - 1;  // consumer warps
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + NS * LY::STAGE_BYTES);
-    uint64_t* empty = full + NS;
-    const int32_t nchunks = (a.n + L - 1) / L;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < NS; ++st) {
-            mbar_init(&full[st], 1);
-            mbar_init(&empty[st], CONSUMERS);
-        }
-        mbar_fence_init();
-    }
-    __syncthreads();  // the only CTA-wide barrier: barriers initialised
-
-    if (warp == 0) {
-        // ---- producer ----
-        if (lane != 0) return;
-        int32_t issued_lo = 0, j = 0;  // chunks [issued_lo, j) issued and possibly unconsumed
-        for (;; ++j) {
-            const int32_t k = blockIdx.x + j * gridDim.x;
-            if (k >= nchunks) break;
-            const int st = j % NS;
-            if (j >= NS) {
-                if (!mbar_wait(&empty[st], (uint32_t)(((j / NS) - 1) & 1))) {
-                    if (a.status) atomicExch(a.status, WT_ERR_TIMEOUT);
-                    break;
-                }
-                issued_lo = j - NS + 1;
-            }
-            if (!stream_issue<PREC, L>(a, smem + (size_t)st * LY::STAGE_BYTES, &full[st], k)) continue;
-        }
-        // keep the CTA's shared memory alive until every issued copy has landed (bounded)
-        for (int32_t q = issued_lo; q < j; ++q) {
-            const int32_t k = blockIdx.x + q * gridDim.x;
-            if (k + 1 == a.test_skip_chunk) continue;
-            mbar_wait(&full[q % NS], (uint32_t)((q / NS) & 1));
-        }
-        return;
-    }
-
-    // ---- consumers ----
-    // Consumer thread ct owns CPT consecutive cells of each chunk (L = 32 * CONSUMERS * CPT),
-    // so a warp reads and writes contiguous runs; with CPT = 2 loads and stores are pairs.
-    static_assert(L == 32 * CONSUMERS * CPT, "chunk = consumer threads x cells per thread");
-    static_assert(L % 32 == 0, "chunk starts at a warp boundary (outlet shuffle)");
-    const int ct = threadIdx.x - 32;
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-#pragma unroll 1
-    for (int32_t j = 0;; ++j) {
-        const int32_t k = blockIdx.x + j * gridDim.x;
-        if (k >= nchunks) break;
-        const int st = j % NS;
-        if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((j / NS) & 1)))) {
-            // the stage never filled: report and leave (the tunnel is invalid until reset)
-            if (a.status && lane == 0) atomicExch(a.status, WT_ERR_TIMEOUT);
-            return;
-        }
-        const unsigned char* stage = smem + (size_t)st * LY::STAGE_BYTES;
-        const uint8_t* codes = stage + Q * LY::POP_BYTES;
-        const int32_t c0 = k * L;
-        const int32_t len = min(L, a.n - c0);
-        const int32_t c = ct * CPT;
-        const bool valid = c < len;  // len is a multiple of 16, so all CPT cells are in range
-        T mx = (T)0.0, my = (T)0.0, mz = (T)0.0, mr = (T)1.0;  // macro values of the latest cell
-        int32_t idx = 0, x = 0, y = 0, z = 0;
-        bool face_row = true;
-        uint32_t code = 0;
-        if (valid) {
-            idx = c0 + c;
-            const int32_t row = (int32_t)a.dnx.div((uint32_t)idx);
-            x = idx - row * nx;  // nx is a multiple of CPT: the cells share the row
-            z = (int32_t)a.dny.div((uint32_t)row);
-            y = row - z * ny;
-            face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
-            const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-            if constexpr (CPT == 1) code = lds(codes + c);
-            else code = lds(reinterpret_cast<const uint16_t*>(codes + c));
-            if (!face_row && x > 0 && x + CPT < nx && code == 0) {
-                T f[CPT][Q];
-                unroll<0, Q>([&](auto ic) {
-                    constexpr int i = decltype(ic)::value;
-                    const S* sp = reinterpret_cast<const S*>(stage + i * LY::POP_BYTES) + a.chunk_r[i] + c;
-                    if constexpr (CPT == 1) {
-                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
-                    } else if constexpr (cx(i) == 0) {  // chunk_r[i] == 0: an aligned pair
-                        const SVec<S, 2> v = lds_pair(sp);
-                        f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
-                        f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
-                    } else {
-                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
-                        f[1][i] = ld_in_smem<P, FAST, i>(sp + 1);
-                    }
-                });
-#pragma unroll
-                for (int q = 0; q < CPT; ++q) {
-                    collide_any<P, FAST>(f[q], x + q, nx, a.tau, a.csmag, mx, my, mz, mr);
-                    if (a.mac_all || row_shell || x + q == 1 || x + q == nx - 2)
-                        store_mac(a.mac_cur, idx + q, mx, my, mz, mr);
-                }
-                unroll<0, Q>([&](auto ic) {
-                    constexpr int i = decltype(ic)::value;
-                    if constexpr (CPT == 1) {
-                        st_out<P, FAST, i>(a.dst[i] + idx, f[0][i]);
-                    } else {
-                        SVec<S, 2> v;
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            if constexpr (P::shifted && !FAST) v.v[q] = P::from(f[q][i] - (T)wd(i));
-                            else v.v[q] = P::from(f[q][i]);
-                        }
-                        vstore<S, 2>(a.dst[i] + idx, v);
-                    }
-                });
-            } else {
-#pragma unroll 1
-                for (int q = 0; q < CPT; ++q) {
-                    const uint32_t cq = (code >> (8 * q)) & 0xffu;
-                    if (CPT > 1 && !face_row && x + q == nx - 1)
-                        outlet_cell<P>(a, idx + q, y, z, cq, mx, my, mz, mr);  // neighbour: cell q-1
-                    else
-                        general_cell<P, FAST>(a, idx + q, x + q, y, z, cq, face_row, row_shell, mx, my, mz, mr);
-                }
-            }
-        }
-        if constexpr (CPT == 1) {
-            // outlet: chunk starts are multiples of 32 and the outlet index is odd, so its
-            // x = nx-2 neighbour is the previous lane
-            const T qx = __shfl_up_sync(0xffffffffu, mx, 1);
-            const T qy = __shfl_up_sync(0xffffffffu, my, 1);
-            const T qz = __shfl_up_sync(0xffffffffu, mz, 1);
-            const T qr = __shfl_up_sync(0xffffffffu, mr, 1);
-            if (valid && !face_row && x == nx - 1) outlet_cell<P>(a, idx, y, z, code, qx, qy, qz, qr);
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[st]);  // this warp is done with the stage
-    }
-}
 
 // Tile variants of the step kernel. Direct-load forms (kind 0): cells per thread (V),
 // threads per block, minimum resident blocks per SM (bounds registers). Streaming forms
@@ -962,15 +13,6 @@ struct StepVariant {
     int (*launch)(const void* args, int32_t n, cudaStream_t st);
 };
 
-static int num_sms() {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-    }
-    return sms;
-}
 
 template <int PREC, bool FAST, int V, int BLOCK, int MINB>
 static int launch_bulk(const void* args, int32_t n, cudaStream_t st) {

@@ -21,7 +21,9 @@ COLLIDE_EXACT, COLLIDE_FAST = 0, 1
 # every symbol include/wt.h declares (tests check that the library exports them all)
 EXPORTS = ['wt_last_error', 'wt_abi_version', 'wt_check_dims', 'wt_population_bytes', 'wt_init_eq',
            'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step_tiles', 'wt_step',
-           'wt_reduce_scratch_len', 'wt_forces', 'wt_forces_noalloc', 'wt_mass', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp']
+           'wt_reduce_scratch_len', 'wt_forces', 'wt_forces_noalloc', 'wt_mass', 'wt_batch_workspace_bytes',
+           'wt_batch_create', 'wt_batch_step', 'wt_batch_capture', 'wt_batch_replay', 'wt_batch_cur',
+           'wt_batch_destroy', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp']
 
 
 class WtError(RuntimeError):
@@ -68,6 +70,13 @@ def lib():
             'wt_forces': ([gp, i32, vp, vp, i64, vp, vp, vp], ctypes.c_int),
             'wt_forces_noalloc': ([gp, i32, vp, vp, i64, vp, vp], ctypes.c_int),
             'wt_mass': ([gp, i32, vp, vp, vp], ctypes.c_int),
+            'wt_batch_workspace_bytes': ([gp, i32, i32], i64),
+            'wt_batch_create': ([gp, i32, vp, vp, vp, vp, i32, vp, i64, vp, ctypes.POINTER(vp)], ctypes.c_int),
+            'wt_batch_step': ([vp, i32, i32, vp], ctypes.c_int),
+            'wt_batch_capture': ([vp, i32, i32, vp], ctypes.c_int),
+            'wt_batch_replay': ([vp, vp], ctypes.c_int),
+            'wt_batch_cur': ([vp, vp], ctypes.c_int),
+            'wt_batch_destroy': ([vp], ctypes.c_int),
             'wt_advect': ([vp, vp, vp, vp, i32, i32, i32, i64, f32, f32, f32, u32, f32, f32, f32, f32, f32, vp],
                           ctypes.c_int),
             'wt_pack_particles': ([vp, vp, vp, vp, i32, i32, i32, i64, vp], ctypes.c_int),
