@@ -16,6 +16,11 @@ reset, then K frames each with its outputs read back to pinned host memory). Pop
 
 N > 1 runs independent replicas, one tunnel per GPU ("replicas only": independent
 tunnels never exchange data); time is the max over ranks.
+
+At N = 1 the line also carries `serving`: the config-5 serving loop (Poisson sessions of
+0.5-33.5M cells under a 160 GB budget, 30 frames/s requested per session) run from its
+stationary population for `--serving` seconds per storage precision, with p50/p99 frame
+latency, admitted sessions and aggregate GLUPS.
 """
 import argparse
 import json
@@ -28,6 +33,9 @@ import time
 
 import numpy as np
 
+# many sessions of uneven sizes come and go in the serving run: map device memory in
+# growable segments so freed tunnels' memory is reusable by differently sized ones
+os.environ.setdefault('PYTORCH_CUDA_ALLOC_CONF', 'expandable_segments:True')
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, 'wind-tunnel_b200'))
 
@@ -381,6 +389,8 @@ def main():
     ap.add_argument('--no-accuracy', dest='accuracy', action='store_false')
     ap.add_argument('--no-batch', dest='batch', action='store_false')
     ap.add_argument('--accuracy-steps', type=int, default=2000)
+    ap.add_argument('--serving', type=float, default=20.0,
+                    help='seconds of the config-5 serving run per precision (0 = skip; N = 1 only)')
     args = ap.parse_args()
 
     world = env_int('WORLD_SIZE', 1)
@@ -397,6 +407,15 @@ def main():
         dist.init_process_group('nccl', timeout=timedelta(seconds=120),
                                 device_id=torch.device('cuda', local_rank))
     r = run_ours(args, rank, world, local_rank)
+    serving_out = None
+    if world == 1 and args.serving > 0 and args.precision == 'fp32':
+        import serving
+        ms = serving.masks()
+        serving_out = {}
+        for prec in ('fp32', 'fp16'):
+            serving_out[prec] = serving.simulate(duration=args.serving, precision=prec, device=f'cuda:{local_rank}',
+                                                 mask_set=ms)
+            torch.cuda.empty_cache()
     cpu = None
     if rank == 0 and not args.no_cpu:
         import bodies
@@ -421,7 +440,7 @@ def main():
                    'parallelism': f'replicas x{world}'},
         'roofline': r['roofline'], 'cpu_baseline': cpu, 'e2e': r['e2e'], 'clocks': r['clocks'],
         'gpu_launches': r['launches'], 'precision_variants': r['variants'], 'accuracy_vs_fp64': r['accuracy'],
-        'batching': r['batching'],
+        'batching': r['batching'], 'serving': serving_out,
     }
     print(json.dumps(line), flush=True)
 

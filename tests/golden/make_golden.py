@@ -8,9 +8,11 @@ float64) scalars. The outputs are written as small ``.npz`` fixtures beside this
 tests pin the C++ oracle and the CUDA kernels to them.
 
 Usage (needs the reference checkout; the fixtures themselves are committed):
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference            # solver fixtures
+    python tests/golden/make_golden.py /root/reference --frames   # wire frames (frames.npz)
 """
 import hashlib
+import json
 import os
 import sys
 import time
@@ -159,8 +161,63 @@ def case_sphere(K, real, name, steps=100, frames=True):
     np.savez_compressed(os.path.join(HERE, name), **out)
 
 
+def load_app(ref, K):
+    """The reference server module (server/app.py) imported with the stub warp and the
+    reference solver module bound to its names; only its pure ``pack`` is used."""
+    import importlib.util
+    saved = {k: sys.modules.get(k) for k in ('warp', 'lbm')}
+    sys.modules['warp'], sys.modules['lbm'] = K.wp, K.mod
+    try:
+        spec = importlib.util.spec_from_file_location('_ref_app', os.path.join(ref, 'server', 'app.py'))
+        app = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(app)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                del sys.modules[k]
+            else:
+                sys.modules[k] = v
+    return app
+
+
+def frames(ref):
+    """Frames written by the reference's own ``pack`` (server/app.py:23-41) for headers and
+    parts shaped like the Engine's (server/app.py:179-193): every combination of parts the
+    Engine sends, odd part sizes so the 8-byte padding is exercised."""
+    K = RefKernels(ref, np.float32)
+    app = load_app(ref, K)
+    rng = np.random.default_rng(21)
+    cases = [  # (numP, slice (w, h) or None, numVerts)
+        (13, (12, 7), 5), (2000, None, 0), (0, (33, 9), 0), (0, None, 0), (5, None, 301)]
+    out = {}
+    for k, (num_p, wh, nv) in enumerate(cases):
+        header = {'type': 'frame', 'dims': [64, 28, 36], 'numP': num_p, 'numVerts': nv,
+                  'forces': [float(v) for v in rng.normal(size=3) * 1e-2], 'steps': int(rng.integers(1, 40)),
+                  'mlups': float(rng.uniform(0, 5e4)), 'running': bool(k % 2 == 0)}
+        parts = []
+        if num_p:
+            parts.append(('parts16', rng.integers(0, 65536, 4 * num_p).astype(np.uint16)))
+            parts.append(('parts8', rng.integers(0, 256, num_p).astype(np.uint8)))
+        if wh:
+            parts.append(('slice', rng.integers(0, 256, 2 * wh[0] * wh[1]).astype(np.uint8)))
+            header.update(sliceW=wh[0], sliceH=wh[1], sliceAxis=k % 3)
+        if nv:
+            parts.append(('cp', rng.integers(-128, 128, nv).astype(np.int8)))
+        data = app.pack(header, parts)
+        out[f'frame_{k}'] = np.frombuffer(data, np.uint8)
+        out[f'header_{k}'] = np.frombuffer(json.dumps(header).encode(), np.uint8)
+        out[f'names_{k}'] = np.array([n for n, _ in parts] or [''])
+        for name, arr in parts:
+            out[f'{name}_{k}'] = arr
+    out['cases'] = np.array(len(cases))
+    np.savez_compressed(os.path.join(HERE, 'frames.npz'), **out)
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    if '--frames' in sys.argv:
+        frames(ref)
+        return
     t0 = time.time()
     meta = {}
     for real, tag in ((np.float32, 'f32'), (np.float64, 'f64')):

@@ -53,7 +53,14 @@ class TunnelBatch:
         for s, c in zip(self.solvers, cur):
             s.cur = int(c)
 
+    def _wait_members(self):
+        # work queued on the member Solvers' own streams (frame kernels reading the
+        # populations and mac) comes before the batch overwrites them
+        for s in self.solvers:
+            self.stream.wait_stream(s.stream)
+
     def step(self, steps, mac_all_last=True):
+        self._wait_members()
         call('wt_batch_step', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
         self._sync_cur()
 
@@ -61,7 +68,15 @@ class TunnelBatch:
         call('wt_batch_capture', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
 
     def replay(self):
+        self._wait_members()
         call('wt_batch_replay', self.handle, self.sh)
+
+    def event(self):
+        """A CUDA event recorded after the work queued so far on the batch stream; member
+        Solvers wait on it (Solver.wait_event) before their frame kernels."""
+        e = torch.cuda.Event()
+        e.record(self.stream)
+        return e
 
     def synchronize(self):
         self.stream.synchronize()

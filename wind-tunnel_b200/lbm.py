@@ -15,6 +15,7 @@ import ctypes
 import numpy as np
 import torch
 
+import wire
 import wtlib as W
 from wtlib import call, ptr
 
@@ -46,6 +47,17 @@ def bytes_per_cell(precision='fp32'):
 
 # The reference's name for the admission footprint (server/lbm.py:30, used by app.py:76).
 BYTES_PER_CELL = bytes_per_cell('fp32')
+
+
+def estimate_bytes(dims, precision='fp32', particles=0, num_verts=0):
+    """Device bytes of a Solver before it exists: the per-cell state, particle buffers
+    (pos 16 + speed 4 + packed 9 bytes each, twice the packed bytes for the frame buffer),
+    the slice buffer and the force partials. The link list (8 bytes per fluid cell next to a
+    wall) is not included; Solver.device_bytes() gives the exact figure afterwards."""
+    nx, ny, nz = (int(d) for d in dims)
+    slice_max = max(nx * ny, nx * nz, nz * ny)
+    return (bytes_per_cell(precision) * nx * ny * nz + particles * (20 + 2 * 9) + 2 * 2 * slice_max
+            + num_verts * 26 + 8 * int(W.lib().wt_reduce_scratch_len(0)) + 4096)
 
 
 def _device(device):
@@ -187,9 +199,18 @@ class Solver:
             call('wt_step', self.gp, self.cur, steps, float(p['uIn']), float(p['tau']), float(p['smag']),
                  W.STEP_MAC_ALL_LAST, self.sh)
             self.cur ^= steps & 1
+        self.advance_particles(steps, p)
+
+    def advance_particles(self, steps, p):
+        """The particle half of step(): one RK2 advection over dt = steps with a fresh seed.
+        A tunnel stepped inside a TunnelBatch calls this after the batch's steps."""
         if self.num_p and steps:
             self.seed += 1
             self._advect(float(steps), p)
+
+    def wait_event(self, event):
+        """Make this Solver's stream wait for a CUDA event (e.g. a TunnelBatch's steps)."""
+        self.stream.wait_event(event)
 
     def _advect(self, dt, p):
         self._require_float_mac('particles')
@@ -271,6 +292,64 @@ class Solver:
         self.launch_frame(p, want_cp)
         return self.collect_frame()
 
+    def launch_frame_packed(self, p, want_cp):
+        """The frame kernels of launch_frame, writing straight into one device buffer laid out
+        as the wire payload (wire.FrameLayout), the six force components in its 48-byte tail,
+        then one device-to-host copy into pinned memory. Nothing waits; collect_frame_packed()
+        returns the frame bytes the reference's pack() would send (server/app.py:179-193)."""
+        sl = p.get('slice')
+        slice_on = bool(sl) and sl.get('field', -1) >= 0
+        cp_on = bool(want_cp) and self.num_verts > 0
+        wh = self.slice_dims(int(sl['axis'])) if slice_on else None
+        layout = wire.FrameLayout(self.num_p, wh, self.num_verts if cp_on else 0)
+        if getattr(self, '_pk_layout_key', None) != (self.num_p, wh, layout.total_bytes):
+            with torch.cuda.stream(self.stream):
+                self._pk_dev = torch.zeros(layout.total_bytes, dtype=torch.uint8, device=self.dev)
+            self._pk_host = torch.empty(layout.total_bytes, dtype=torch.uint8, pin_memory=True)
+            self._pk_layout_key = (self.num_p, wh, layout.total_bytes)
+        base = self._pk_dev.data_ptr()
+        mac = self.mac[self.cur]
+        extra = {}
+        if self.num_p:
+            self._require_float_mac('particles')
+            call('wt_pack_particles', ptr(self.pos), ptr(self.spd), base + layout.offsets['parts16'],
+                 base + layout.offsets['parts8'], self.nx, self.ny, self.nz, self.num_p, self.sh)
+        if slice_on:
+            self._require_float_mac('slice')
+            axis = int(sl['axis'])
+            dim = (self.nx, self.ny, self.nz)[axis]
+            index = max(0, min(dim - 1, int(sl['index'])))
+            call('wt_slice', ptr(mac), ptr(self.solid), base + layout.offsets['slice'], self.nx, self.ny, self.nz,
+                 axis, index, int(sl['field']), float(p['uIn']), float(p['lref']), float(sl['vmin']),
+                 float(sl['vmax']), self.sh)
+            extra = {'sliceW': wh[0], 'sliceH': wh[1], 'sliceAxis': axis}
+        if cp_on:
+            self._require_float_mac('surface pressure')
+            call('wt_cp', ptr(mac), ptr(self.solid), ptr(self.verts), ptr(self.norms), base + layout.offsets['cp'],
+                 self.nx, self.ny, self.nz, self.num_verts, float(p['uIn']), CP_RANGE, self.sh)
+        call('wt_forces', self.gp, self.cur, ptr(self.link_cells), ptr(self.link_masks), self.n_links,
+             ptr(self.partials), base + layout.forces_offset, self.sh)
+        with torch.cuda.stream(self.stream):
+            self._pk_host.copy_(self._pk_dev, non_blocking=True)
+            self._pk_event = torch.cuda.Event()
+            self._pk_event.record(self.stream)
+        self._pk_pending = (layout, extra)
+
+    def collect_frame_packed(self, header):
+        """Wait for launch_frame_packed's copy and return the frame bytes. ``header`` holds
+        the Engine's keys in its order (type, dims, numP, numVerts, forces, steps, mlups,
+        running); forces and the slice keys are filled in here."""
+        layout, extra = self._pk_pending
+        self._pk_pending = None
+        self._pk_event.synchronize()
+        host = self._pk_host.numpy()
+        f6 = host[layout.forces_offset:layout.forces_offset + 48].view(np.float64)
+        self.last_forces6 = f6.copy()
+        h = dict(header)
+        h['forces'] = [float(v) for v in f6[:3]]
+        h.update(extra)
+        return layout.frame(h, host)
+
     # ---- extras used by tests, the serving loop and the benchmark ----
     def forces6(self):
         """[Fx, Fy, Fz] over all solid==1 links, then without links into the y = 0 plane (fp64)."""
@@ -300,6 +379,17 @@ class Solver:
 
     def synchronize(self):
         self.stream.synchronize()
+
+    def device_bytes(self):
+        """Bytes of device memory this Solver holds (its tensors; the caching allocator's
+        rounding and the frame buffer's reuse come on top)."""
+        ts = [*self.f, *self.mac, self.solid, self.code, self.forces_dev, self.mass_dev, self.status_dev,
+              self.partials, self.slice_buf, self.link_cells, self.link_masks]
+        for k in ('pos', 'spd', 'q16', 'q8', 'verts', 'norms', 'cp_buf', '_pk_dev'):
+            t = getattr(self, k, None)
+            if t is not None:
+                ts.append(t)
+        return sum(t.numel() * t.element_size() for t in ts)
 
     def status(self, clear=True):
         """Device status word: 0, or wtlib.WT_ERR_TIMEOUT if a kernel's bounded wait gave up

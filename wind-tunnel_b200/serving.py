@@ -1,0 +1,357 @@
+"""Multi-session serving loop: the reference's Engine thread (server/app.py:150-202) turned
+into a request loop with continuous batching.
+
+The reference runs one tunnel shared by every client, steps it from a 60 Hz loop and sends a
+frame to the clients whose previous frame has been acknowledged (`ready`). Here each session
+owns a tunnel on one GPU:
+
+* **Admission.** A session is admitted in arrival order once its device footprint
+  (``lbm.estimate_bytes``: populations, mac, mask, particle and frame buffers) fits in what
+  the HBM budget has left. Later arrivals queue behind it. A session whose lifetime ends
+  while it still waits leaves the queue (counted as abandoned).
+* **Requests.** A session's client asks for its first frame on admission and for each next
+  one when it has its previous frame and its 1/fps tick has come: the reference's `ready`
+  flow control (server/app.py:173-193) with 30 fps pacing.
+* **Rounds.** A round takes every session with an outstanding request. Their tunnels advance
+  ``steps_per_frame`` steps together in one ``TunnelBatch`` (one persistent bulk kernel per
+  step over a tile work-list that spans every tunnel, then one face kernel); the batch is
+  rebuilt only when the set of sessions changes. Then each session's stream waits for the
+  batch, advects its particles and runs its frame kernels, which write the wire-format frame
+  straight into one device buffer (``Solver.launch_frame_packed``), and one copy brings it
+  back. Frames are collected in session order. Sessions admitted while a round runs join
+  the next round, so their work overlaps everyone else's from then on.
+* **Latency.** A frame's latency runs from its request to the moment its bytes are on the
+  host. ``stats()`` gives p50/p99 over all frames, admitted/retired/abandoned/queued counts,
+  the peak and end memory in use, and the aggregate lattice-update rate over the window.
+
+Under oversubscription (more cells than the GPU can step at 30 x steps_per_frame per second)
+every session is due in every round, frames come as fast as the GPU allows, and the frame
+latency equals the round time: steps_per_frame x cells in service / throughput.
+"""
+import argparse
+import heapq
+import json
+import time
+
+import numpy as np
+
+import bodies
+import lbm
+
+
+class Session:
+    """One client's tunnel: its grid, mask and parameters (the Engine's `p` dict,
+    server/app.py:61-63), its lifetime and its request clock."""
+
+    def __init__(self, sid, dims, solid, params, lifetime, particles=5000, frontal=None, arrival=0.0):
+        self.id = sid
+        self.dims = tuple(int(d) for d in dims)
+        nx, ny, nz = self.dims
+        self.n = nx * ny * nz
+        self.solid = solid
+        self.p = dict(maxAge=2.2 * nx / (params['uIn'] * 10), lref=40.0, seedX=2.0, seedCy=(ny - 1) / 2,
+                      seedCz=(nz - 1) / 2, seedHy=(ny - 4) / 2, seedHz=(nz - 4) / 2,
+                      slice=dict(axis=1, index=ny // 2, field=0, vmin=0.0, vmax=1.6))
+        self.p.update(params)
+        self.particles = int(particles)
+        self.lifetime = float(lifetime)
+        self.arrival = float(arrival)
+        self.frontal = frontal if frontal is not None else bodies.areas(solid, self.dims)[0]
+        self.solver = None
+        self.bytes = 0
+        self.request_t = None
+        self.admitted_t = None
+        self.last_t = None
+        self.frames = 0
+        self.steps = 0
+        self.cd = self.cl = float('nan')
+        self.last_frame = None
+
+
+class SessionServer:
+    """Admission, rounds and latency accounting for many sessions on one GPU.
+
+    ``solver_factory(session)`` returns a ready Solver (mask, equilibrium, particles) and
+    ``batch_factory(solvers, params)`` a TunnelBatch; ``footprint(session)`` the bytes
+    admission charges. The defaults build lbm.Solver / batch.TunnelBatch on ``device``.
+    ``clock`` is the time source (seconds)."""
+
+    def __init__(self, device='cuda:0', budget_bytes=160e9, precision='fp32', fps=30.0, steps_per_frame=10,
+                 tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
+                 footprint=None, keep_frames=False):
+        self.device = device
+        self.budget = float(budget_bytes)
+        self.precision = precision
+        self.collision = collision
+        self.period = 1.0 / fps
+        self.steps_per_frame = int(steps_per_frame)
+        self.tile = int(tile)
+        self.clock = clock
+        self.solver_factory = solver_factory or self._make_solver
+        self.batch_factory = batch_factory or self._make_batch
+        self.footprint = footprint or (lambda s: lbm.estimate_bytes(s.dims, precision, s.particles))
+        self.keep_frames = keep_frames
+        self.active = {}          # id -> Session, in admission order
+        self.queue = []           # FIFO of sessions waiting for memory
+        self.used = 0.0
+        self.peak_used = 0.0
+        self.latencies = []
+        self.frame_log = []       # (session id, frame bytes) when keep_frames
+        self.cell_updates = 0
+        self.t0 = None
+        self.rounds = 0
+        self.rebuilds = 0
+        self.max_active = 0
+        self.active_sum = 0
+        self.max_queued = 0
+        self.admitted = self.retired = self.abandoned = 0
+        self._batch = None
+        self._batch_key = None
+        self._stream = None
+
+    # ---- default factories (the GPU path) ----
+    def _make_solver(self, s):
+        sv = lbm.Solver(s.dims, self.device, precision=self.precision, collision=self.collision, seed=s.id)
+        sv.set_solid(s.solid)
+        sv.reset(s.p['uIn'])
+        if s.particles:
+            sv.set_particles(s.particles, s.p)
+        return sv
+
+    def _make_batch(self, solvers, params):
+        import torch
+        from batch import TunnelBatch
+        if self._stream is None:
+            self._stream = torch.cuda.Stream(torch.device(self.device))
+        return TunnelBatch(solvers, params, tile=self.tile, stream=self._stream)
+
+    # ---- admission ----
+    def submit(self, session):
+        self.queue.append(session)
+        self.max_queued = max(self.max_queued, len(self.queue))
+
+    def _admit(self, now):
+        while self.queue:
+            s = self.queue[0]
+            if now - s.arrival >= s.lifetime:  # the client gave up while waiting
+                self.queue.pop(0)
+                self.abandoned += 1
+                continue
+            need = self.footprint(s)
+            if self.used + need > self.budget:
+                break
+            self.queue.pop(0)
+            s.solver = self.solver_factory(s)
+            s.bytes = max(need, s.solver.device_bytes())
+            s.admitted_t = s.request_t = s.last_t = now
+            self.used += s.bytes
+            self.peak_used = max(self.peak_used, self.used)
+            self.active[s.id] = s
+            self.admitted += 1
+        self.max_active = max(self.max_active, len(self.active))
+
+    def _retire(self, now):
+        gone = [s for s in self.active.values() if now - s.arrival >= s.lifetime]
+        if not gone:
+            return
+        if self._batch is not None and any(s.id in self._batch_key for s in gone):
+            self._batch.close()
+            self._batch, self._batch_key = None, None
+        for s in gone:
+            del self.active[s.id]
+            self.used -= s.bytes
+            s.solver.synchronize()
+            s.solver = None
+            self.retired += 1
+
+    # ---- one round ----
+    def round(self):
+        """Retire, admit, then serve every session with an outstanding request. Returns the
+        number of frames produced."""
+        now = self.clock()
+        if self.t0 is None:
+            self.t0 = now
+        self._retire(now)
+        self._admit(now)
+        due = [s for s in self.active.values() if s.request_t <= now]
+        if not due:
+            return 0
+        key = tuple(s.id for s in due)
+        if key != self._batch_key:
+            if self._batch is not None:
+                self._batch.close()
+            self._batch = self.batch_factory([s.solver for s in due], [s.p for s in due])
+            self._batch_key = key
+            self.rebuilds += 1
+        k = self.steps_per_frame
+        self._batch.step(k)
+        done = self._batch.event()
+        for s in due:
+            s.solver.wait_event(done)
+            s.solver.advance_particles(k, s.p)
+            s.solver.launch_frame_packed(s.p, False)
+        for s in due:
+            sv = s.solver
+            header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=0, forces=None, steps=k,
+                          mlups=0.0, running=True)
+            t_prev = s.last_t
+            frame = sv.collect_frame_packed(header)
+            t = self.clock()
+            self.latencies.append(t - s.request_t)
+            if self.keep_frames:
+                self.frame_log.append((s.id, frame))
+            s.last_frame = frame
+            s.frames += 1
+            s.steps += k
+            s.last_t = t
+            self.cell_updates += s.n * k
+            fx, fy = float(sv.last_forces6[0]), float(sv.last_forces6[1])
+            q = 0.5 * s.p['uIn'] ** 2 * max(1, s.frontal)  # the client's Cd/Cl (web/js/main.js:337-339)
+            s.cd, s.cl = fx / q, fy / q
+            s.mlups = s.n * k / max(1e-9, t - t_prev) / 1e6
+            # the client acknowledges at once and asks again at its next 1/fps tick
+            s.request_t = max(t, s.request_t + self.period)
+        self.rounds += 1
+        self.active_sum += len(self.active)
+        return len(due)
+
+    def stats(self):
+        now = self.clock()
+        lat = np.array(self.latencies) * 1e3 if self.latencies else np.zeros(1)
+        span = max(1e-9, now - (self.t0 if self.t0 is not None else now))
+        return {'frames': len(self.latencies), 'p50_ms': round(float(np.percentile(lat, 50)), 2),
+                'p99_ms': round(float(np.percentile(lat, 99)), 2), 'max_ms': round(float(lat.max()), 2),
+                'rounds': self.rounds, 'batch_rebuilds': self.rebuilds, 'admitted': self.admitted,
+                'retired': self.retired, 'abandoned': self.abandoned, 'active_end': len(self.active),
+                'max_active': self.max_active,
+                'mean_active': round(self.active_sum / max(1, self.rounds), 1), 'queued_end': len(self.queue),
+                'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
+                'peak_used_gb': round(self.peak_used / 1e9, 2),
+                'glups': round(self.cell_updates / span / 1e9, 3),
+                'frames_per_session_s': round(len(self.latencies) / span / max(1e-9, self.active_sum / max(1, self.rounds)), 2)}
+
+    def reset_window(self):
+        """Start a fresh measurement window (drop latencies and counters so far)."""
+        self.latencies.clear()
+        self.cell_updates = 0
+        self.rounds = self.active_sum = 0
+        self.t0 = self.clock()
+
+    def close(self):
+        if self._batch is not None:
+            self._batch.close()
+            self._batch, self._batch_key = None, None
+        for s in self.active.values():
+            s.solver.synchronize()
+        self.active.clear()
+
+
+# ---- config 5: Poisson arrivals of tunnels of four sizes ----
+SIZES = {0.5e6: (128, 64, 64), 2e6: (200, 100, 100), 8e6: (320, 160, 160), 33.5e6: (512, 256, 256)}
+PROBS = (0.4, 0.3, 0.2, 0.1)
+
+
+def masks(per_size=2, seed=55):
+    """Seeded ellipsoid-union obstacles (1-6 ellipsoids on a moving belt) for each size,
+    with their frontal areas: {size: [(solid, frontal), ...]}."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = {}
+    for size, dims in SIZES.items():
+        out[size] = []
+        for _ in range(per_size):
+            solid, _ = bodies.ellipsoid_union(dims, int(rng.integers(1, 7)), int(rng.integers(1 << 31)),
+                                              scale=dims[0] / 512.0, floor='belt')
+            out[size].append((solid, bodies.areas(solid, dims)[0]))
+    return out
+
+
+class Arrivals:
+    """Session generator for config 5: sizes {0.5, 2, 8, 33.5}M cells with probabilities
+    {0.4, 0.3, 0.2, 0.1}, u0 uniform in [0.03, 0.08], nu uniform in [0.001, 0.01]
+    (tau = 3 nu + 1/2), Cs = 0.16, exponential lifetimes, all from one PCG64 stream."""
+
+    def __init__(self, seed=5, mean_life=60.0, particles=5000, mask_set=None):
+        self.rng = np.random.Generator(np.random.PCG64(seed))
+        self.mean_life = mean_life
+        self.particles = particles
+        self.masks = mask_set if mask_set is not None else masks()
+        self.sizes = list(SIZES)
+        self.next_id = 0
+
+    def session(self, now):
+        size = self.sizes[int(self.rng.choice(len(self.sizes), p=PROBS))]
+        dims = SIZES[size]
+        solid, frontal = self.masks[size][self.next_id % len(self.masks[size])]
+        u0 = float(self.rng.uniform(0.03, 0.08))
+        nu = float(self.rng.uniform(0.001, 0.01))
+        s = Session(self.next_id, dims, solid, dict(uIn=u0, tau=3 * nu + 0.5, smag=0.16),
+                    lifetime=float(self.rng.exponential(self.mean_life)), particles=self.particles,
+                    frontal=frontal, arrival=now)
+        self.next_id += 1
+        return s
+
+
+def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='fp32', seed=5, device='cuda:0',
+             particles=5000, warm_start=True, tile=0, steps_per_frame=10, fps=30.0, mask_set=None):
+    """Config 5 in wall-clock time: Poisson arrivals at `rate` per second for `duration`
+    seconds, each session requesting `fps` frames per second of its particles, one slice and
+    Cd/Cl, admitted against `budget` bytes. With warm_start the run begins from the arrival
+    process's stationary population (Poisson with mean rate x mean_life sessions; lifetimes
+    are memoryless, so their residual lifetimes are exponential with the same mean), so the
+    window measures the steady state; the set-up of those sessions is not timed."""
+    gen = Arrivals(seed, mean_life, particles, mask_set)
+    srv = SessionServer(device, budget_bytes=budget, precision=precision, fps=fps,
+                        steps_per_frame=steps_per_frame, tile=tile)
+    start = time.perf_counter()
+    if warm_start:
+        for _ in range(int(gen.rng.poisson(rate * mean_life))):
+            srv.submit(gen.session(start))
+        srv._admit(start)
+    setup_s = time.perf_counter() - start
+    t0 = time.perf_counter()
+    for s in srv.active.values():  # the window starts now; set-up time is not service time
+        s.arrival += t0 - start
+        s.admitted_t = s.request_t = s.last_t = t0
+    for s in srv.queue:
+        s.arrival += t0 - start
+    arrivals, t = [], t0
+    while True:
+        t += float(gen.rng.exponential(1.0 / rate))
+        if t > t0 + duration:
+            break
+        heapq.heappush(arrivals, t)
+    srv.reset_window()
+    while time.perf_counter() < t0 + duration:
+        now = time.perf_counter()
+        while arrivals and arrivals[0] <= now:
+            srv.submit(gen.session(heapq.heappop(arrivals)))
+        if srv.round() == 0:
+            time.sleep(0.0005)
+    out = srv.stats()
+    out.update(precision=precision, duration_s=duration, arrival_rate=rate, mean_lifetime_s=mean_life,
+               budget_gb=budget / 1e9, warm_start=warm_start, steps_per_frame=steps_per_frame, fps=fps,
+               particles=particles, setup_s=round(setup_s, 1))
+    srv.close()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description='Config 5 serving simulation (Poisson sessions on one GPU)')
+    ap.add_argument('--duration', type=float, default=300.0)
+    ap.add_argument('--rate', type=float, default=2.0)
+    ap.add_argument('--mean-life', type=float, default=60.0)
+    ap.add_argument('--budget-gb', type=float, default=160.0)
+    ap.add_argument('--precision', nargs='+', default=['fp32', 'fp16'])
+    ap.add_argument('--steps-per-frame', type=int, default=10)
+    ap.add_argument('--tile', type=int, default=0)
+    ap.add_argument('--seed', type=int, default=5)
+    a = ap.parse_args(argv)
+    ms = masks()
+    for prec in a.precision:
+        r = simulate(a.duration, a.rate, a.mean_life, a.budget_gb * 1e9, prec, a.seed, tile=a.tile,
+                     steps_per_frame=a.steps_per_frame, mask_set=ms)
+        print(json.dumps(r), flush=True)
+
+
+if __name__ == '__main__':
+    main()
