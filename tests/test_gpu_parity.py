@@ -17,6 +17,11 @@ from conftest import golden
 pytestmark = pytest.mark.gpu
 
 RANDOM_CASES = ['random_12x8x10', 'random_4x4x4', 'random_28x6x5']
+# D3Q19 velocities and weights in the reference's order (server/lbm.py:15-18)
+C = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1), (1, 1, 0), (-1, -1, 0),
+     (1, -1, 0), (-1, 1, 0), (1, 0, 1), (-1, 0, -1), (1, 0, -1), (-1, 0, 1), (0, 1, 1), (0, -1, -1), (0, 1, -1),
+     (0, -1, 1)]
+W = [1 / 3] + [1 / 18] * 6 + [1 / 36] * 12
 TAGS = {'f32': ('fp32', np.float32, torch.float32), 'f64': ('fp64', np.float64, torch.float64)}
 
 
@@ -271,6 +276,46 @@ def test_fast_collision_matches_oracle(oracle_mod, prec_name, oprec, dims):
         err = np.abs(got - ref).max()
         assert err <= FAST_ATOL[prec_name], f'{prec_name} tile {tile}: max |df| {err}'
         np.testing.assert_allclose(s.macro(), L.mac.astype(np.float64), atol=20 * FAST_ATOL[prec_name], rtol=0)
+
+
+def _random_flow(s, seed, umax=0.3):
+    """Equilibrium populations at random rho in [0.95, 1.05] and velocities uniform in
+    [-umax, umax]^3 (|u| up to 0.52: some cells hit the 0.35 clamp, their neighbours not)."""
+    rng = np.random.default_rng(seed)
+    c = np.array(C, np.float64)
+    w = np.array(W, np.float64)
+    u = rng.uniform(-umax, umax, (s.n, 3))
+    rho = rng.uniform(0.95, 1.05, s.n)
+    cu = u @ c.T
+    f = (w[None, :] * rho[:, None] * (1 + 3 * cu + 4.5 * cu * cu - 1.5 * (u * u).sum(1)[:, None])).T
+    if s.precision in (1, 2):  # shifted storage
+        f = f - w[:, None]
+    _load(s, s.cur, f.reshape(-1))
+
+
+@pytest.mark.parametrize('prec_name', ['fp32', 'fp16', 'bf16'])
+@pytest.mark.parametrize('dims', [(64, 24, 20), (48, 9, 7)])
+def test_fast_pair_collision_same_bits_in_every_tile(prec_name, dims):
+    """Tiles with two or four cells per thread run the fast collision on cell pairs with
+    sm_100's paired fp32 instructions, which round each lane like the one-lane forms: every
+    tile must give the bits of the one-cell tile, including cells whose pair partner is
+    clamped, in the outlet sponge or next to a wall."""
+    import autotune
+    solid = _random_case(dims, 29)
+    p = dict(uIn=0.07, tau=0.512, smag=0.16)
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name, collision='fast')
+    tiles = [t[0] for t in autotune.admissible(s)]
+    assert 1 in tiles and any(t[1] >= 2 for t in autotune.admissible(s))
+    out = {}
+    for tile in [1] + [t for t in tiles if t != 1]:
+        s.set_tile(tile)
+        s.reset(p['uIn'])
+        s.cur = 0
+        _random_flow(s, 5)
+        s.step(3, p)
+        out[tile] = (s.populations(), s.macro())
+        assert np.array_equal(out[tile][0], out[1][0]), f'{prec_name} tile {tile}: populations'
+        assert np.array_equal(out[tile][1], out[1][1]), f'{prec_name} tile {tile}: mac'
 
 
 def test_fast_collision_close_to_exact():

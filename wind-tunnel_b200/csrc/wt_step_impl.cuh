@@ -321,6 +321,69 @@ __device__ __forceinline__ float rsqrt_fast(float x) {  // x > 0
 }
 __device__ __forceinline__ double rsqrt_fast(double x) { return 1.0 / sqrt(x); }
 
+// Two cells in one register pair. sm_100's paired fp32 instructions (FADD2, FMUL2, FFMA2)
+// round each lane to nearest like the one-lane forms, so collide_fast on F2 gives each of
+// the two cells exactly the bits of collide_fast on float, in about half the instructions.
+struct F2 {
+    float2 v;
+    F2() = default;
+    __device__ __forceinline__ explicit F2(double s) : v(make_float2((float)s, (float)s)) {}
+    __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { F2 r; r.v = __fadd2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ F2 operator-(F2 a) { return F2(-a.v.x, -a.v.y); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return a + (-b); }  // x - y == x + (-y) in IEEE
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { F2 r; r.v = __fmul2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ F2 fmaT(F2 a, F2 b, F2 c) { F2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r; }
+__device__ __forceinline__ F2 rcp_fast(F2 x) {
+    float r0, r1;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(x.v.x));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(x.v.y));
+    const F2 r(r0, r1);
+    return fmaT(r, fmaT(-x, r, F2(1.0)), r);
+}
+__device__ __forceinline__ F2 sqrt_fast(F2 x) { return F2(sqrt_fast(x.v.x), sqrt_fast(x.v.y)); }
+__device__ __forceinline__ F2 rsqrt_fast(F2 x) {
+    float r0, r1;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(x.v.x));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(x.v.y));
+    const F2 r(r0, r1);
+    return r * (F2(1.5) - (F2(0.5) * x) * (r * r));
+}
+// a > t in any lane; lane-wise a > t ? p : q
+__device__ __forceinline__ bool any_gt(float a, float t) { return a > t; }
+__device__ __forceinline__ bool any_gt(double a, double t) { return a > t; }
+__device__ __forceinline__ bool any_gt(F2 a, F2 t) { return a.v.x > t.v.x || a.v.y > t.v.y; }
+__device__ __forceinline__ float sel_gt(float a, float t, float p, float q) { return a > t ? p : q; }
+__device__ __forceinline__ double sel_gt(double a, double t, double p, double q) { return a > t ? p : q; }
+__device__ __forceinline__ F2 sel_gt(F2 a, F2 t, F2 p, F2 q) {
+    return F2(a.v.x > t.v.x ? p.v.x : q.v.x, a.v.y > t.v.y ? p.v.y : q.v.y);
+}
+// x coordinate of the cell(s): x, or (x, x + 1) for a pair
+template <class T>
+__device__ __forceinline__ T xcoord(int32_t x) { return (T)x; }
+template <>
+__device__ __forceinline__ F2 xcoord<F2>(int32_t x) { return F2((float)x, (float)(x + 1)); }
+
+// B = rho (1 - 1.5 u.u) - tr(A)/3 (with S for rho where SHIFT). The pair form evaluates it one
+// lane at a time: compiled on F2 inside the full collision, this one expression came out a
+// last-bit different from the one-cell form in about 0.5% of cells (though its F2 form alone
+// matches), and per-lane evaluation restores identical bits at a cost of a few instructions.
+template <class T, bool SHIFT>
+struct BTerm {
+    __device__ static __forceinline__ T eval(T rho, T S, T usq, T axx, T ayy, T azz) {
+        const T tra3 = ((axx + ayy) + azz) * (T)(1.0 / 3.0);
+        return fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+    }
+};
+template <bool SHIFT>
+struct BTerm<F2, SHIFT> {
+    __device__ static __forceinline__ F2 eval(F2 rho, F2 S, F2 usq, F2 axx, F2 ayy, F2 azz) {
+        return F2(BTerm<float, SHIFT>::eval(rho.v.x, S.v.x, usq.v.x, axx.v.x, ayy.v.x, azz.v.x),
+                  BTerm<float, SHIFT>::eval(rho.v.y, S.v.y, usq.v.y, axx.v.y, ayy.v.y, azz.v.y));
+    }
+};
+
 template <class T, bool SHIFT>
 __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy,
                                              T& ouz, T& orho) {
@@ -344,28 +407,27 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
     const T ir = rcp_fast(rho);
     T ux = jx * ir, uy = jy * ir, uz = jz * ir;
     T usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
-    if (usq > (T)0.1225) {  // |u| > 0.35 (server/lbm.py:131-135)
-        const T sc = (T)0.35 * rsqrt_fast(usq);
+    if (any_gt(usq, (T)0.1225)) {  // |u| > 0.35 (server/lbm.py:131-135)
+        // a lane below the limit scales by 1 (exact) and recomputes the same usq
+        const T sc = sel_gt(usq, (T)0.1225, (T)0.35 * rsqrt_fast(usq), (T)1.0);
         ux = ux * sc; uy = uy * sc; uz = uz * sc;
         usq = fmaT(uz, uz, fmaT(uy, uy, ux * ux));
     }
     const T rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
-    const T t3 = (SHIFT ? S : rho) * ((T)1.0 / (T)3.0);
+    const T t3 = (SHIFT ? S : rho) * (T)(1.0 / 3.0);  // the float nearest 1/3 either way
     const T nxx = fmaT(-rux, ux, xxx - t3), nyy = fmaT(-ruy, uy, xyy - t3), nzz = fmaT(-ruz, uz, xzz - t3);
     const T nxy = fmaT(-rux, uy, xxy), nxz = fmaT(-rux, uz, xxz), nyz = fmaT(-ruy, uz, xyz);
     const T q1 = fmaT(nzz, nzz, fmaT(nyy, nyy, nxx * nxx));
     const T q2 = fmaT(nyz, nyz, fmaT(nxz, nxz, nxy * nxy));
     const T qn = sqrt_fast(fmaT((T)2.0, q2, q1));
-    T tau0 = tau;
-    const T sp = (T)x - (T)(nx - 24);  // outlet sponge (server/lbm.py:149-151)
-    if (sp > (T)0.0) tau0 = fmaT(sp, (T)0.015, tau);
+    const T sp = xcoord<T>(x) - (T)(nx - 24);  // outlet sponge (server/lbm.py:149-151)
+    const T tau0 = sel_gt(sp, (T)0.0, fmaT(sp, (T)0.015, tau), tau);
     const T tau_e = (T)0.5 * (tau0 + sqrt_fast(fmaT(tau0, tau0, csmag * qn * ir)));
     const T keep = (T)1.0 - rcp_fast(tau_e);
     const T k45 = (T)4.5 * keep, k9 = (T)9.0 * keep;
     const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
     const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;  // 2 A_ab
-    const T tra3 = ((axx + ayy) + azz) * ((T)1.0 / (T)3.0);
-    const T B = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+    const T B = BTerm<T, SHIFT>::eval(rho, S, usq, axx, ayy, azz);
     const T w0 = (T)wd(0), w1 = (T)wd(1), w2 = (T)wd(7);
     const T w1x3 = (T)(3.0 * wd(1)), w2x3 = (T)(3.0 * wd(7));
     v[0] = w0 * B;
@@ -533,6 +595,76 @@ __device__ __forceinline__ void outlet_cell(const StepArgs<typename P::S, typena
 // V consecutive cells starting at idx0 (a multiple of V, and idx0 % 32 is the lane's
 // multiple of V, so for V == 1 the previous cell is the previous lane). All 32 lanes of a
 // warp must call this together (the V == 1 outlet exchanges values by shuffle).
+// Collision of V consecutive plain fluid cells of one row, with their mac stores in cell
+// order; the fast float form takes the cells two at a time on F2 (bit-identical per cell).
+// mx..mr end as the last cell's macro values.
+template <class P, bool FAST, int V>
+__device__ __forceinline__ void collide_cells(const StepArgs<typename P::S, typename P::T>& a,
+                                              typename P::T (&f)[V][Q], int32_t idx0, int32_t x0, bool row_shell,
+                                              typename P::T& mx, typename P::T& my, typename P::T& mz,
+                                              typename P::T& mr) {
+    using T = typename P::T;
+    const int32_t nx = a.nx;
+    if constexpr (FAST && V % 2 == 0 && std::is_same<T, float>::value) {
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            F2 g[Q];
+#pragma unroll
+            for (int i = 0; i < Q; ++i) g[i] = F2(f[k][i], f[k + 1][i]);
+            F2 ux, uy, uz, rho;
+            collide_fast<F2, P::shifted>(g, x0 + k, nx, F2(a.tau), F2(a.csmag), ux, uy, uz, rho);
+#pragma unroll
+            for (int i = 0; i < Q; ++i) {
+                f[k][i] = g[i].v.x;
+                f[k + 1][i] = g[i].v.y;
+            }
+            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2)
+                store_mac(a.mac_cur, idx0 + k, ux.v.x, uy.v.x, uz.v.x, rho.v.x);
+            mx = ux.v.y; my = uy.v.y; mz = uz.v.y; mr = rho.v.y;
+            if (a.mac_all || row_shell || x0 + k + 1 == 1 || x0 + k + 1 == nx - 2)
+                store_mac(a.mac_cur, idx0 + k + 1, mx, my, mz, mr);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, mx, my, mz, mr);
+            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2) store_mac(a.mac_cur, idx0 + k, mx, my, mz, mr);
+        }
+    }
+}
+
+// Population I of V consecutive cells to p (aligned to V elements); half-width storage
+// rounds two values per conversion (each to nearest, as one at a time).
+template <class P, bool FAST, int V, int I>
+__device__ __forceinline__ void store_cells(typename P::S* p, const typename P::T (&f)[V][Q]) {
+    using S = typename P::S;
+    using T = typename P::T;
+    if constexpr (V == 1) {
+        st_out<P, FAST, I>(p, f[0][I]);
+    } else {
+        SVec<S, V> v;
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            T lo = f[k][I], hi = f[k + 1][I];
+            if constexpr (P::shifted && !FAST) {
+                lo = lo - (T)wd(I);
+                hi = hi - (T)wd(I);
+            }
+            if constexpr (std::is_same<S, __half>::value) {
+                const __half2 h = __floats2half2_rn(lo, hi);
+                memcpy(&v.v[k], &h, 4);
+            } else if constexpr (std::is_same<S, __nv_bfloat16>::value) {
+                const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+                memcpy(&v.v[k], &h, 4);
+            } else {
+                v.v[k] = P::from(lo);
+                v.v[k + 1] = P::from(hi);
+            }
+        }
+        vstore<S, V>(p, v);
+    }
+}
+
 template <int PREC, bool FAST, int V>
 __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                            int32_t idx0, bool valid) {
@@ -577,24 +709,10 @@ __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S
                 }
             }
         });
-#pragma unroll
-        for (int k = 0; k < V; ++k) {
-            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, mx, my, mz, mr);
-            if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2) store_mac(a.mac_cur, idx0 + k, mx, my, mz, mr);
-        }
+        collide_cells<P, FAST, V>(a, f, idx0, x0, row_shell, mx, my, mz, mr);
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            if constexpr (V == 1) {
-                st_out<P, FAST, i>(a.dst[i] + idx0, f[0][i]);
-            } else {
-                SVec<S, V> v;
-#pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    if constexpr (P::shifted && !FAST) v.v[k] = P::from(f[k][i] - (T)wd(i));
-                    else v.v[k] = P::from(f[k][i]);
-                }
-                vstore<S, V>(a.dst[i] + idx0, v);
-            }
+            store_cells<P, FAST, V, i>(a.dst[i] + idx0, f);
         });
     } else if (valid) {
         // ---- general path: cell by cell (faces, inlet, outlet, solids, cells next to solids) ----
@@ -924,25 +1042,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
                         f[1][i] = ld_in_smem<P, FAST, i>(sp + 1);
                     }
                 });
-#pragma unroll
-                for (int q = 0; q < CPT; ++q) {
-                    collide_any<P, FAST>(f[q], x + q, nx, a.tau, a.csmag, mx, my, mz, mr);
-                    if (a.mac_all || row_shell || x + q == 1 || x + q == nx - 2)
-                        store_mac(a.mac_cur, idx + q, mx, my, mz, mr);
-                }
+                collide_cells<P, FAST, CPT>(a, f, idx, x, row_shell, mx, my, mz, mr);
                 unroll<0, Q>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
-                    if constexpr (CPT == 1) {
-                        st_out<P, FAST, i>(a.dst[i] + idx, f[0][i]);
-                    } else {
-                        SVec<S, 2> v;
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            if constexpr (P::shifted && !FAST) v.v[q] = P::from(f[q][i] - (T)wd(i));
-                            else v.v[q] = P::from(f[q][i]);
-                        }
-                        vstore<S, 2>(a.dst[i] + idx, v);
-                    }
+                    store_cells<P, FAST, CPT, i>(a.dst[i] + idx, f);
                 });
             } else {
 #pragma unroll 1

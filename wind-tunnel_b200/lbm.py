@@ -292,21 +292,35 @@ class Solver:
         self.launch_frame(p, want_cp)
         return self.collect_frame()
 
+    def _frame_buffers(self, layout, wh):
+        key = (self.num_p, wh, layout.total_bytes)
+        if getattr(self, '_pk_layout_key', None) != key:
+            with torch.cuda.stream(self.stream):
+                self._pk_dev = torch.zeros(layout.total_bytes, dtype=torch.uint8, device=self.dev)
+            self._pk_host = torch.empty(layout.total_bytes, dtype=torch.uint8, pin_memory=True)
+            self._pk_layout_key = key
+
+    def _frame_layout(self, p, want_cp):
+        sl = p.get('slice')
+        slice_on = bool(sl) and sl.get('field', -1) >= 0
+        cp_on = bool(want_cp) and self.num_verts > 0
+        wh = self.slice_dims(int(sl['axis'])) if slice_on else None
+        return wire.FrameLayout(self.num_p, wh, self.num_verts if cp_on else 0), wh, slice_on, cp_on
+
+    def prepare_frame(self, p, want_cp=False):
+        """Allocate the device and pinned host buffers of launch_frame_packed ahead of the
+        first frame (pinned host allocation is slow)."""
+        layout, wh, _, _ = self._frame_layout(p, want_cp)
+        self._frame_buffers(layout, wh)
+
     def launch_frame_packed(self, p, want_cp):
         """The frame kernels of launch_frame, writing straight into one device buffer laid out
         as the wire payload (wire.FrameLayout), the six force components in its 48-byte tail,
         then one device-to-host copy into pinned memory. Nothing waits; collect_frame_packed()
         returns the frame bytes the reference's pack() would send (server/app.py:179-193)."""
+        layout, wh, slice_on, cp_on = self._frame_layout(p, want_cp)
+        self._frame_buffers(layout, wh)
         sl = p.get('slice')
-        slice_on = bool(sl) and sl.get('field', -1) >= 0
-        cp_on = bool(want_cp) and self.num_verts > 0
-        wh = self.slice_dims(int(sl['axis'])) if slice_on else None
-        layout = wire.FrameLayout(self.num_p, wh, self.num_verts if cp_on else 0)
-        if getattr(self, '_pk_layout_key', None) != (self.num_p, wh, layout.total_bytes):
-            with torch.cuda.stream(self.stream):
-                self._pk_dev = torch.zeros(layout.total_bytes, dtype=torch.uint8, device=self.dev)
-            self._pk_host = torch.empty(layout.total_bytes, dtype=torch.uint8, pin_memory=True)
-            self._pk_layout_key = (self.num_p, wh, layout.total_bytes)
         base = self._pk_dev.data_ptr()
         mac = self.mac[self.cur]
         extra = {}

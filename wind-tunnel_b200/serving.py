@@ -108,6 +108,8 @@ class SessionServer:
         self._batch = None
         self._batch_key = None
         self._stream = None
+        self.phase = {'admit': 0.0, 'rebuild': 0.0, 'issue': 0.0, 'collect': 0.0}
+        self.round_s = []
 
     # ---- default factories (the GPU path) ----
     def _make_solver(self, s):
@@ -116,6 +118,8 @@ class SessionServer:
         sv.reset(s.p['uIn'])
         if s.particles:
             sv.set_particles(s.particles, s.p)
+        sv.prepare_frame(s.p, False)
+        sv.synchronize()
         return sv
 
     def _make_batch(self, solvers, params):
@@ -173,8 +177,10 @@ class SessionServer:
             self.t0 = now
         self._retire(now)
         self._admit(now)
+        t_admit = self.clock()
         due = [s for s in self.active.values() if s.request_t <= now]
         if not due:
+            self.phase['admit'] += t_admit - now
             return 0
         key = tuple(s.id for s in due)
         if key != self._batch_key:
@@ -183,6 +189,7 @@ class SessionServer:
             self._batch = self.batch_factory([s.solver for s in due], [s.p for s in due])
             self._batch_key = key
             self.rebuilds += 1
+        t_rebuild = self.clock()
         k = self.steps_per_frame
         self._batch.step(k)
         done = self._batch.event()
@@ -190,6 +197,7 @@ class SessionServer:
             s.solver.wait_event(done)
             s.solver.advance_particles(k, s.p)
             s.solver.launch_frame_packed(s.p, False)
+        t_issue = self.clock()
         for s in due:
             sv = s.solver
             header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=0, forces=None, steps=k,
@@ -211,6 +219,11 @@ class SessionServer:
             s.mlups = s.n * k / max(1e-9, t - t_prev) / 1e6
             # the client acknowledges at once and asks again at its next 1/fps tick
             s.request_t = max(t, s.request_t + self.period)
+        t_end = self.clock()
+        for name, a, b in (('admit', now, t_admit), ('rebuild', t_admit, t_rebuild), ('issue', t_rebuild, t_issue),
+                           ('collect', t_issue, t_end)):
+            self.phase[name] += b - a
+        self.round_s.append(t_end - now)
         self.rounds += 1
         self.active_sum += len(self.active)
         return len(due)
@@ -218,6 +231,7 @@ class SessionServer:
     def stats(self):
         now = self.clock()
         lat = np.array(self.latencies) * 1e3 if self.latencies else np.zeros(1)
+        rs = np.array(self.round_s) * 1e3 if self.round_s else np.zeros(1)
         span = max(1e-9, now - (self.t0 if self.t0 is not None else now))
         return {'frames': len(self.latencies), 'p50_ms': round(float(np.percentile(lat, 50)), 2),
                 'p99_ms': round(float(np.percentile(lat, 99)), 2), 'max_ms': round(float(lat.max()), 2),
@@ -228,11 +242,15 @@ class SessionServer:
                 'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
                 'peak_used_gb': round(self.peak_used / 1e9, 2),
                 'glups': round(self.cell_updates / span / 1e9, 3),
+                'round_ms': {'p50': round(float(np.percentile(rs, 50)), 1), 'p99': round(float(np.percentile(rs, 99)), 1),
+                             **{f'{k}_mean': round(v / max(1, self.rounds) * 1e3, 2) for k, v in self.phase.items()}},
                 'frames_per_session_s': round(len(self.latencies) / span / max(1e-9, self.active_sum / max(1, self.rounds)), 2)}
 
     def reset_window(self):
         """Start a fresh measurement window (drop latencies and counters so far)."""
         self.latencies.clear()
+        self.round_s.clear()
+        self.phase = dict.fromkeys(self.phase, 0.0)
         self.cell_updates = 0
         self.rounds = self.active_sum = 0
         self.t0 = self.clock()
@@ -307,6 +325,7 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
         for _ in range(int(gen.rng.poisson(rate * mean_life))):
             srv.submit(gen.session(start))
         srv._admit(start)
+        srv.round()  # the stationary sessions have been running: one round builds their batch
     setup_s = time.perf_counter() - start
     t0 = time.perf_counter()
     for s in srv.active.values():  # the window starts now; set-up time is not service time
