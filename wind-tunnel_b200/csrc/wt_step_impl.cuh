@@ -633,6 +633,54 @@ __device__ __forceinline__ void collide_cells(const StepArgs<typename P::S, type
     }
 }
 
+// Face equilibrium populations from (br, bux, buy, buz), the values face_eq stores, in the form
+// store_cells takes them: deviations f - w for the fast form of shifted storage, else f.
+template <class P, bool FAST>
+__device__ __forceinline__ void eq_values(typename P::T br, typename P::T bux, typename P::T buy, typename P::T buz,
+                                          typename P::T (&out)[Q]) {
+    using T = typename P::T;
+    const T bsq = (T)1.5 * (bux * bux + buy * buy + buz * buz);
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        T s = (T)0.0;
+        if constexpr (cx(i) > 0) s = s + bux;
+        if constexpr (cx(i) < 0) s = s - bux;
+        if constexpr (cy(i) > 0) s = s + buy;
+        if constexpr (cy(i) < 0) s = s - buy;
+        if constexpr (cz(i) > 0) s = s + buz;
+        if constexpr (cz(i) < 0) s = s - buz;
+        const T bc = (T)3.0 * s;
+        const T v = (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq);
+        if constexpr (P::shifted && FAST) out[i] = v - (T)wd(i);
+        else out[i] = v;
+    });
+}
+
+// Collision of two cells of one row (pair form for the fast float collision); m[k] gets
+// cell k's macro values (ux, uy, uz, rho). No mac stores.
+template <class P, bool FAST>
+__device__ __forceinline__ void collide_two(const StepArgs<typename P::S, typename P::T>& a, typename P::T (&f)[2][Q],
+                                            int32_t x0, typename P::T (&m)[2][4]) {
+    using T = typename P::T;
+    if constexpr (FAST && std::is_same<T, float>::value) {
+        F2 g[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = F2(f[0][i], f[1][i]);
+        F2 ux, uy, uz, rho;
+        collide_fast<F2, P::shifted>(g, x0, a.nx, F2(a.tau), F2(a.csmag), ux, uy, uz, rho);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            f[0][i] = g[i].v.x;
+            f[1][i] = g[i].v.y;
+        }
+        m[0][0] = ux.v.x; m[0][1] = uy.v.x; m[0][2] = uz.v.x; m[0][3] = rho.v.x;
+        m[1][0] = ux.v.y; m[1][1] = uy.v.y; m[1][2] = uz.v.y; m[1][3] = rho.v.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) collide_any<P, FAST>(f[k], x0 + k, a.nx, a.tau, a.csmag, m[k][0], m[k][1], m[k][2], m[k][3]);
+    }
+}
+
 // Population I of V consecutive cells to p (aligned to V elements); half-width storage
 // rounds two values per conversion (each to nearest, as one at a time).
 template <class P, bool FAST, int V, int I>
@@ -665,6 +713,109 @@ __device__ __forceinline__ void store_cells(typename P::S* p, const typename P::
     }
 }
 
+// Two cells (x0 even) of an interior row, whatever their kind, in one lane-uniform sequence:
+// vector pull of both, bounce-back at links into non-fluid cells (server/lbm.py:110-124),
+// one pair collision, then the inlet (x = 0) and outlet (x = nx-1, from its x = nx-2
+// neighbour's values of this step, server/lbm.py:87-107) take face equilibria; a solid cell's
+// populations are not written. The results and mac writes are those of general_cell and
+// outlet_cell, but a warp no longer splits into per-cell branches at walls and row ends.
+template <int PREC, bool FAST>
+__device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                              int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
+                                              bool row_shell) {
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    using S = typename P::S;
+    const int32_t nx = a.nx;
+    const uint32_t c0 = codes & 0xffu, c1 = (codes >> 8) & 0xffu;
+    const bool sol0 = (c0 & CODE_SOLID) != 0, sol1 = (c1 & CODE_SOLID) != 0;
+    const bool inlet = x0 == 0, outlet = x0 + 1 == nx - 1;
+    // mac rule of a solid cell (general_cell) and of the outlet (outlet_cell)
+    const bool wsol0 = a.mac_all || row_shell || x0 == 1 || x0 == nx - 2;
+    const bool wsol1 = outlet ? a.mac_all : (a.mac_all || row_shell || x0 + 1 == 1 || x0 + 1 == nx - 2);
+    if (sol0 && sol1) {
+        if (wsol0) store_mac(a.mac_cur, idx0, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
+        if (wsol1) store_mac(a.mac_cur, idx0 + 1, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
+        return;
+    }
+    // pull: every source of an interior row lies inside the lattice
+    T f[2][Q];
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const S* p = a.src[i] + idx0;
+        const SVec<S, 2> v = vload<S, 2>(p + cx(i));  // aligned: the shift cancels
+        if constexpr (cx(i) == 0) {
+            f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
+            f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
+        } else if constexpr (cx(i) > 0) {
+            f[0][i] = ld_in<P, FAST, i>(p);
+            f[1][i] = ld_in<P, FAST, i>(&v.v[0]);
+        } else {
+            f[0][i] = ld_in<P, FAST, i>(&v.v[1]);
+            f[1][i] = ld_in<P, FAST, i>(p + 1);
+        }
+    });
+    if ((c0 | c1) & CODE_NEAR) {
+        unroll<1, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            const int32_t off = cx(i) + cy(i) * a.nx + cz(i) * a.nxy;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (((k ? c1 : c0) & CODE_NEAR) == 0) continue;
+                const int t = a.solid[idx0 + k - off];
+                if (t != 0) {
+                    // bounce-back; in deviation form w_opp(i) = w_i, so the value carries over
+                    T b = ld_in<P, FAST, opp(i)>(a.fin + (int64_t)opp(i) * a.n + idx0 + k);
+                    if constexpr (cx(i) != 0) {
+                        if (t == 2) b = b + (T)(6.0 * wd(i) * cx(i)) * a.uin;
+                    }
+                    f[k][i] = b;
+                }
+            }
+        });
+    }
+    T m[2][4];
+    collide_two<P, FAST>(a, f, x0, m);
+    if (sol0) {  // a solid cell's macro values are (0, 0, 0, 1); the outlet may read them
+        m[0][0] = (T)0.0; m[0][1] = (T)0.0; m[0][2] = (T)0.0; m[0][3] = (T)1.0;
+    }
+    if (inlet && !sol0) {
+        eq_values<P, FAST>((T)1.0, a.uin, (T)0.0, (T)0.0, f[0]);
+        m[0][0] = a.uin; m[0][1] = (T)0.0; m[0][2] = (T)0.0; m[0][3] = (T)1.0;
+    }
+    if (outlet && !sol1) {
+        T br, bux, buy, buz;
+        face_values<T>(nx - 1, y, z, nx, a.ny, a.nz, a.uin, m[0][0], m[0][1], m[0][2], m[0][3], br, bux, buy, buz);
+        eq_values<P, FAST>(br, bux, buy, buz, f[1]);
+        m[1][0] = bux; m[1][1] = buy; m[1][2] = buz; m[1][3] = br;
+    }
+    if (!sol0 && !sol1) {
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            store_cells<P, FAST, 2, i>(a.dst[i] + idx0, f);
+        });
+    } else {
+        const int32_t k = sol0 ? 1 : 0;  // the one fluid cell of the pair (selects, no indexing)
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            st_out<P, FAST, i>(a.dst[i] + idx0 + k, sol0 ? f[1][i] : f[0][i]);
+        });
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool sol = k ? sol1 : sol0;
+        const int32_t x = x0 + k;
+        bool w;
+        if (sol) w = k ? wsol1 : wsol0;
+        else if (x == 0 || x == nx - 1) w = a.mac_all;  // inlet / outlet
+        else w = a.mac_all || row_shell || x == 1 || x == nx - 2;
+        if (w) {
+            if (sol) store_mac(a.mac_cur, idx0 + k, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
+            else store_mac(a.mac_cur, idx0 + k, m[k][0], m[k][1], m[k][2], m[k][3]);
+        }
+    }
+}
+
 template <int PREC, bool FAST, int V>
 __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                            int32_t idx0, bool valid) {
@@ -684,6 +835,12 @@ __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S
         if constexpr (V == 4) codes = *reinterpret_cast<const uint32_t*>(a.code + idx0);
         else if constexpr (V == 2) codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
         else codes = a.code[idx0];
+    }
+    if constexpr (V == 2) {
+        if (valid && !face_row) {
+            interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell);
+            return;
+        }
     }
     if (valid && !face_row && x0 > 0 && x0 + V <= nx - 2 + (V == 1) && codes == 0) {
         // ---- fast path: V plain interior fluid cells, vector loads and stores ----
