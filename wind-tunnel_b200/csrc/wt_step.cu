@@ -56,7 +56,11 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     {10, 1, 1, 1024, 1, 992, 2, launch_stream<PREC, FAST, 992, 2, 1024, 1, 1>},          \
     {11, 1, 2, 512, 1, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 1, 2>},            \
     {12, 1, 1, 512, 2, 480, 4, launch_stream<PREC, FAST, 480, 4, 512, 2, 1>},            \
-    {13, 1, 2, 512, 2, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 2, 2>}
+    {13, 1, 2, 512, 2, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 2, 2>},            \
+    {14, 1, 2, 512, 1, 960, 3, launch_stream<PREC, FAST, 960, 3, 512, 1, 2>},            \
+    {15, 1, 2, 512, 1, 960, 4, launch_stream<PREC, FAST, 960, 4, 512, 1, 2>},            \
+    {16, 1, 2, 256, 2, 448, 4, launch_stream<PREC, FAST, 448, 4, 256, 2, 2>},            \
+    {17, 1, 2, 384, 1, 704, 4, launch_stream<PREC, FAST, 704, 4, 384, 1, 2>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants(int* count) {

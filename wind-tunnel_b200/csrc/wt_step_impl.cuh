@@ -713,24 +713,65 @@ __device__ __forceinline__ void store_cells(typename P::S* p, const typename P::
     }
 }
 
+// Raw stored values of the pull of one pair of cells (x0 even) of an interior row: for each
+// population the aligned two-element vector at p + cx(i) and, where cx(i) != 0, the one
+// element outside it; plus the pair's code bytes.
+template <class S>
+struct PairRaw {
+    SVec<S, 2> v[Q];
+    S e[Q];
+    uint32_t codes;
+};
+
+// every source of an interior row lies inside the lattice
+template <int PREC>
+__device__ __forceinline__ void pair_load(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                          int32_t idx0, PairRaw<typename Prec<PREC>::S>& r) {
+    using S = typename Prec<PREC>::S;
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const S* p = a.src[i] + idx0;
+        r.v[i] = vload<S, 2>(p + cx(i));  // aligned: the shift cancels
+        if constexpr (cx(i) > 0) r.e[i] = p[0];
+        if constexpr (cx(i) < 0) r.e[i] = p[1];
+    });
+    r.codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
+}
+
+template <class P, bool FAST>
+__device__ __forceinline__ void pair_unpack(const PairRaw<typename P::S>& r, typename P::T (&f)[2][Q]) {
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (cx(i) == 0) {
+            f[0][i] = ld_in<P, FAST, i>(&r.v[i].v[0]);
+            f[1][i] = ld_in<P, FAST, i>(&r.v[i].v[1]);
+        } else if constexpr (cx(i) > 0) {
+            f[0][i] = ld_in<P, FAST, i>(&r.e[i]);
+            f[1][i] = ld_in<P, FAST, i>(&r.v[i].v[0]);
+        } else {
+            f[0][i] = ld_in<P, FAST, i>(&r.v[i].v[1]);
+            f[1][i] = ld_in<P, FAST, i>(&r.e[i]);
+        }
+    });
+}
+
 // Two cells (x0 even) of an interior row, whatever their kind, in one lane-uniform sequence:
 // vector pull of both, bounce-back at links into non-fluid cells (server/lbm.py:110-124),
 // one pair collision, then the inlet (x = 0) and outlet (x = nx-1, from its x = nx-2
 // neighbour's values of this step, server/lbm.py:87-107) take face equilibria; a solid cell's
 // populations are not written. The results and mac writes are those of general_cell and
 // outlet_cell, but a warp no longer splits into per-cell branches at walls and row ends.
+// pair_finish takes the pulled populations; interior_pair loads them itself.
 template <int PREC, bool FAST>
-__device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
-                                              int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
-                                              bool row_shell) {
+__device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                            int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
+                                            bool row_shell, typename Prec<PREC>::T (&f)[2][Q]) {
     using P = Prec<PREC>;
     using T = typename P::T;
-    using S = typename P::S;
     const int32_t nx = a.nx;
     const uint32_t c0 = codes & 0xffu, c1 = (codes >> 8) & 0xffu;
     const bool sol0 = (c0 & CODE_SOLID) != 0, sol1 = (c1 & CODE_SOLID) != 0;
     const bool inlet = x0 == 0, outlet = x0 + 1 == nx - 1;
-    // mac rule of a solid cell (general_cell) and of the outlet (outlet_cell)
     const bool wsol0 = a.mac_all || row_shell || x0 == 1 || x0 == nx - 2;
     const bool wsol1 = outlet ? a.mac_all : (a.mac_all || row_shell || x0 + 1 == 1 || x0 + 1 == nx - 2);
     if (sol0 && sol1) {
@@ -738,23 +779,6 @@ __device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>
         if (wsol1) store_mac(a.mac_cur, idx0 + 1, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
         return;
     }
-    // pull: every source of an interior row lies inside the lattice
-    T f[2][Q];
-    unroll<0, Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        const S* p = a.src[i] + idx0;
-        const SVec<S, 2> v = vload<S, 2>(p + cx(i));  // aligned: the shift cancels
-        if constexpr (cx(i) == 0) {
-            f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
-            f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
-        } else if constexpr (cx(i) > 0) {
-            f[0][i] = ld_in<P, FAST, i>(p);
-            f[1][i] = ld_in<P, FAST, i>(&v.v[0]);
-        } else {
-            f[0][i] = ld_in<P, FAST, i>(&v.v[1]);
-            f[1][i] = ld_in<P, FAST, i>(p + 1);
-        }
-    });
     if ((c0 | c1) & CODE_NEAR) {
         unroll<1, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
@@ -814,6 +838,22 @@ __device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>
             else store_mac(a.mac_cur, idx0 + k, m[k][0], m[k][1], m[k][2], m[k][3]);
         }
     }
+}
+
+template <int PREC, bool FAST>
+__device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                              int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
+                                              bool row_shell) {
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    const bool sol0 = (codes & CODE_SOLID) != 0, sol1 = ((codes >> 8) & CODE_SOLID) != 0;
+    T f[2][Q];
+    if (!(sol0 && sol1)) {  // an all-solid pair pulls nothing
+        PairRaw<typename P::S> r;
+        pair_load<PREC>(a, idx0, r);
+        pair_unpack<P, FAST>(r, f);
+    }
+    pair_finish<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, f);
 }
 
 template <int PREC, bool FAST, int V>
@@ -1183,7 +1223,23 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
             const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
             if constexpr (CPT == 1) code = lds(codes + c);
             else code = lds(reinterpret_cast<const uint16_t*>(codes + c));
-            if (!face_row && x > 0 && x + CPT < nx && code == 0) {
+            if (CPT == 2 && !face_row) {
+                // every cell kind of an interior row: the pair path (see pair_finish)
+                T f[2][Q];
+                unroll<0, Q>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    const S* sp = reinterpret_cast<const S*>(stage + i * LY::POP_BYTES) + a.chunk_r[i] + c;
+                    if constexpr (cx(i) == 0) {  // chunk_r[i] == 0: an aligned pair
+                        const SVec<S, 2> v = lds_pair(sp);
+                        f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
+                        f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
+                    } else {
+                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
+                        f[1][i] = ld_in_smem<P, FAST, i>(sp + 1);
+                    }
+                });
+                if constexpr (CPT == 2) pair_finish<PREC, FAST>(a, idx, x, y, z, code, row_shell, f);
+            } else if (!face_row && x > 0 && x + CPT < nx && code == 0) {
                 T f[CPT][Q];
                 unroll<0, Q>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
