@@ -33,9 +33,6 @@ import time
 
 import numpy as np
 
-# many sessions of uneven sizes come and go in the serving run: map device memory in
-# growable segments so freed tunnels' memory is reusable by differently sized ones
-os.environ.setdefault('PYTORCH_CUDA_ALLOC_CONF', 'expandable_segments:True')
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, 'wind-tunnel_b200'))
 
@@ -307,7 +304,7 @@ def run_batching(dev, replays=5, graph_steps=100):
     cells = sum(s.n for s in solvers)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tile_ms, steps_done = {}, 0
-    for tile in (1, 2, 3, 7):
+    for tile in (1, 2, 3, 7, 18):
         b = TunnelBatch(solvers, params, tile=tile)
         b.step(2)
         ev0.record(b.stream)

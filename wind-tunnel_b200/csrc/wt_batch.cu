@@ -96,7 +96,8 @@ static void launch_batch_faces(const void* args, int grid, cudaStream_t st) {
     {3, 2, 128, 6, launch_batch_bulk<PREC, FAST, 2, 128, 6>, launch_batch_faces<PREC>},                      \
     {4, 2, 128, 4, launch_batch_bulk<PREC, FAST, 2, 128, 4>, launch_batch_faces<PREC>},                      \
     {5, 4, 128, 4, launch_batch_bulk<PREC, FAST, 4, 128, 4>, launch_batch_faces<PREC>},                      \
-    {7, 2, 256, 3, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>}
+    {7, 2, 256, 3, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>},                      \
+    {18, 2, 128, 8, launch_batch_bulk<PREC, FAST, 2, 128, 8>, launch_batch_faces<PREC>}
 
 template <int PREC, bool FAST>
 static const BatchVariant* batch_variant(int id) {
@@ -145,7 +146,8 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 // tile shape of a batch (direct-load variants only)
 int tile_shape(int32_t tile, int* v, int* block) {
-    static const int ids[][3] = {{1, 1, 256}, {2, 1, 128}, {3, 2, 128}, {4, 2, 128}, {5, 4, 128}, {7, 2, 256}};
+    static const int ids[][3] = {{1, 1, 256}, {2, 1, 128}, {3, 2, 128}, {4, 2, 128}, {5, 4, 128}, {7, 2, 256},
+                                 {18, 2, 128}};
     const int want = tile > 0 ? tile : 2;
     for (const auto& r : ids)
         if (r[0] == want) {

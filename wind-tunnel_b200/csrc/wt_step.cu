@@ -60,7 +60,8 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     {14, 1, 2, 512, 1, 960, 3, launch_stream<PREC, FAST, 960, 3, 512, 1, 2>},            \
     {15, 1, 2, 512, 1, 960, 4, launch_stream<PREC, FAST, 960, 4, 512, 1, 2>},            \
     {16, 1, 2, 256, 2, 448, 4, launch_stream<PREC, FAST, 448, 4, 256, 2, 2>},            \
-    {17, 1, 2, 384, 1, 704, 4, launch_stream<PREC, FAST, 704, 4, 384, 1, 2>}
+    {17, 1, 2, 384, 1, 704, 4, launch_stream<PREC, FAST, 704, 4, 384, 1, 2>},            \
+    {18, 0, 2, 128, 8, 0, 0, launch_bulk<PREC, FAST, 2, 128, 8>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants(int* count) {
@@ -69,13 +70,14 @@ const StepVariant* variants(int* count) {
     return table;
 }
 
-// defaults until the autotuner has measured the tunnel: one cell per thread at 64
-// registers; fp64 needs 128 registers to avoid spills, so two cells per thread there
+// defaults until the autotuner has measured the tunnel: two cells per thread at 64
+// registers (the fastest shape at 33.5M cells in fp32, fp16 and bf16); fp64 needs 128
+// registers to avoid spills, so it keeps two cells per thread at 128 registers
 template <int PREC>
 const StepVariant* pick_variant(const wt_grid* g) {
     int count;
     const StepVariant* t = g->collision == WT_COLLIDE_FAST ? variants<PREC, true>(&count) : variants<PREC, false>(&count);
-    const int want = g->tile > 0 ? g->tile : (PREC == WT_F64 ? 4 : 1);
+    const int want = g->tile > 0 ? g->tile : (PREC == WT_F64 ? 4 : 18);
     for (int k = 0; k < count; ++k) {
         if (t[k].id != want) continue;
         if (g->nx % t[k].v != 0) return nullptr;

@@ -728,9 +728,11 @@ template <int PREC>
 __device__ __forceinline__ void pair_load(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                           int32_t idx0, PairRaw<typename Prec<PREC>::S>& r) {
     using S = typename Prec<PREC>::S;
+    // one per-thread base; the per-population offsets are the same for every thread
+    const S* fb = a.fin + idx0;
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        const S* p = a.src[i] + idx0;
+        const S* p = fb + ((int64_t)i * a.n - (cx(i) + cy(i) * (int64_t)a.nx + cz(i) * (int64_t)a.nxy));
         r.v[i] = vload<S, 2>(p + cx(i));  // aligned: the shift cancels
         if constexpr (cx(i) > 0) r.e[i] = p[0];
         if constexpr (cx(i) < 0) r.e[i] = p[1];
@@ -813,16 +815,17 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
         eq_values<P, FAST>(br, bux, buy, buz, f[1]);
         m[1][0] = bux; m[1][1] = buy; m[1][2] = buz; m[1][3] = br;
     }
+    typename P::S* ob = a.dst[0] + idx0;  // population i of the output is at ob + i n
     if (!sol0 && !sol1) {
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            store_cells<P, FAST, 2, i>(a.dst[i] + idx0, f);
+            store_cells<P, FAST, 2, i>(ob + (int64_t)i * a.n, f);
         });
     } else {
         const int32_t k = sol0 ? 1 : 0;  // the one fluid cell of the pair (selects, no indexing)
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            st_out<P, FAST, i>(a.dst[i] + idx0 + k, sol0 ? f[1][i] : f[0][i]);
+            st_out<P, FAST, i>(ob + (int64_t)i * a.n + k, sol0 ? f[1][i] : f[0][i]);
         });
     }
 #pragma unroll

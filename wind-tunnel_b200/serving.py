@@ -85,7 +85,8 @@ class SessionServer:
         self.collision = collision
         self.period = 1.0 / fps
         self.steps_per_frame = int(steps_per_frame)
-        self.tile = int(tile)
+        # batched tile: two cells per thread at 64 registers unless chosen (fp64 spills there)
+        self.tile = int(tile) if tile else (2 if precision == 'fp64' else 18)
         self.clock = clock
         self.solver_factory = solver_factory or self._make_solver
         self.batch_factory = batch_factory or self._make_batch
