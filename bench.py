@@ -277,7 +277,8 @@ def run_ours(args, rank, world, local_rank):
     acc = None
     if args.accuracy and prec == 'fp32' and rank == 0:
         import accuracy
-        acc = accuracy.study(steps=args.accuracy_steps, scale=0.5, device=dev)
+        acc = {'chaotic_nu0.001': accuracy.study(steps=args.accuracy_steps, scale=0.5, device=dev),
+               'laminar_nu0.02': accuracy.study(steps=2 * args.accuracy_steps, scale=0.5, device=dev, nu=0.02)}
 
     return dict(value=value, t_dev=t_dev, roofline=roofline, e2e=e2e, clocks=clk.summary(), accuracy=acc,
                 batching=batching,
