@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define WT_ABI_VERSION 1
+#define WT_ABI_VERSION 2
 
 enum {
     WT_OK = 0,
@@ -42,13 +42,18 @@ enum {
     WT_ERR_TIMEOUT = -5   /* a bounded device wait gave up */
 };
 
+/* population storage. WT_F16 / WT_BF16 store deviations d_i = f_i - e_i in half width,
+ * e_i = w_i (1 + 3 c_xi U + 4.5 c_xi^2 U^2 - 1.5 U^2), the equilibrium at rho = 1,
+ * u = (U, 0, 0) with U = wt_grid.shift_u (evaluated in double, rounded to float once); near
+ * the free stream the deviations are small, where half precision resolves them finely.
+ * U = 0 gives e_i = w_i. Arithmetic is float in every case. */
 enum { WT_F32 = 0, WT_F16 = 1, WT_BF16 = 2, WT_F64 = 3 };
 
 /* collision forms. EXACT evaluates the reference's expressions in the reference's order
  * (bit-identical to server/lbm.py run serially). FAST evaluates the same regularized
  * Smagorinsky collision in moment space with fused multiply-adds (about 40% fewer
  * operations; equal to EXACT up to rounding); with fp16/bf16 storage it works on the
- * stored deviations f_i - w_i directly. */
+ * stored deviations f_i - e_i directly. */
 enum { WT_COLLIDE_EXACT = 0, WT_COLLIDE_FAST = 1 };
 
 /* wt_step flags */
@@ -68,7 +73,8 @@ typedef struct wt_grid {
     int32_t* status;       /* optional device int: set to WT_ERR_TIMEOUT if a bounded wait gives up */
     int32_t test_skip_chunk; /* test hook for the failure path: 0 = off; k > 0: chunk k-1 of a
                                 streaming tile is never loaded, so its bounded wait expires */
-    int32_t pad_;
+    float shift_u;         /* fp16/bf16 storage shift velocity U (see WT_F16); ignored otherwise.
+                              Must equal the shift_u the buffers were initialised with. */
 } wt_grid;
 
 /* ---- library ---- */
@@ -81,8 +87,10 @@ int64_t wt_population_bytes(int32_t precision, int64_t n);
 
 /* ---- set-up ---- */
 /* init_kernel (server/lbm.py:64-69), launched by Solver.reset (:415-417): equilibrium at
- * rho = 1, u = (uin, 0, 0) into population buffer f, and mac = (uin, 0, 0, 1). */
-int wt_init_eq(int32_t precision, void* f, void* mac, int64_t n, double uin, void* stream);
+ * rho = 1, u = (uin, 0, 0) into population buffer f, and mac = (uin, 0, 0, 1). fp16/bf16
+ * buffers are written relative to the shift at velocity shift_u (wt_grid.shift_u of the
+ * tunnel; uin itself keeps the free stream's deviations near zero). */
+int wt_init_eq(int32_t precision, void* f, void* mac, int64_t n, double uin, double shift_u, void* stream);
 /* Derive the per-cell code byte from solid (after Solver.set_solid, server/lbm.py:419-421). */
 int wt_build_codes(const wt_grid* g, void* stream);
 /* Compacted momentum-exchange link list: every interior fluid cell with at least one

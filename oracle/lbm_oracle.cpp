@@ -77,16 +77,30 @@ struct StF64 { using Store = double; using Real = double; static constexpr bool 
 struct StF16 { using Store = _Float16; using Real = float; static constexpr bool shifted = true; };
 struct StBF16 { using Store = __bf16; using Real = float; static constexpr bool shifted = true; };
 
+// Shift of the fp16/bf16 storage (the library's wt_grid.shift_u, restated): populations are
+// stored as f_i - e_i, e_i = w_i (1 + 3 c_xi U + 4.5 c_xi^2 U^2 - 1.5 U^2) in double rounded to
+// float; bb_i = e_opp(i) - e_i; dw_i = e_i - w_i; su, suu, s45, s15 = U, U^2, 4.5 U^2, 1.5 U^2.
+// U = 0 gives e_i = w_i. Set by oracle_set_shift; applies to every later call.
+struct ShiftState {
+    float e[Q], bb[Q], dw[Q];
+    float su, suu, s45, s15;
+};
+static ShiftState g_shift = [] {
+    ShiftState t{};
+    for (int i = 0; i < Q; ++i) t.e[i] = (float)w_d(i);
+    return t;
+}();
+
 template <class St>
 inline typename St::Real ld(const typename St::Store* f, int64_t n, int i, int64_t idx, const Consts<typename St::Real>& K) {
     using T = typename St::Real;
-    if constexpr (St::shifted) return (T)f[(int64_t)i * n + idx] + K.w[i];
+    if constexpr (St::shifted) return (T)f[(int64_t)i * n + idx] + (T)g_shift.e[i];
     else return (T)f[(int64_t)i * n + idx];
 }
 template <class St>
 inline void st(typename St::Store* f, int64_t n, int i, int64_t idx, typename St::Real v, const Consts<typename St::Real>& K) {
     using S = typename St::Store;
-    if constexpr (St::shifted) f[(int64_t)i * n + idx] = (S)(v - K.w[i]);
+    if constexpr (St::shifted) f[(int64_t)i * n + idx] = (S)(v - (typename St::Real)g_shift.e[i]);
     else f[(int64_t)i * n + idx] = (S)v;
 }
 
@@ -122,10 +136,13 @@ void collide_fast(T (&v)[Q], int x, int nx, T tau, T csmag, T& oux, T& ouy, T& o
     const T s15 = v[15] + v[16], a15 = v[15] - v[16];
     const T s17 = v[17] + v[18], a17 = v[17] - v[18];
     const T d7 = s7 + s9, d11 = s11 + s13, d15 = s15 + s17;
-    const T xxx = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
+    // shifted storage: the shift's own moments (+ U^2 in xx, + U in jx) restored
+    const T xxx0 = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
+    const T xxx = SHIFT ? xxx0 + (T)g_shift.suu : xxx0;
     const T xxy = s7 - s9, xxz = s11 - s13, xyz = s15 - s17;
     const T S = ((v[0] + s1) + (s3 + s5)) + ((d7 + d11) + d15);
-    const T jx = ((a1 + a7) + (a9 + a11)) + a13;
+    const T jx0 = ((a1 + a7) + (a9 + a11)) + a13;
+    const T jx = SHIFT ? jx0 + (T)g_shift.su : jx0;
     const T jy = ((a3 + a7) - (a9 - a15)) + a17;
     const T jz = ((a5 + a11) - (a13 - a15)) - a17;
     const T rho = SHIFT ? S + (T)1.0 : S;
@@ -153,7 +170,12 @@ void collide_fast(T (&v)[Q], int x, int nx, T tau, T csmag, T& oux, T& ouy, T& o
     const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
     const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;
     const T tra3 = ((axx + ayy) + azz) * ((T)1.0 / (T)3.0);
-    const T B = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+    const T B0 = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+    const T B = SHIFT ? B0 + (T)g_shift.s15 : B0;
+    // shifted storage: directions with c_x != 0 lose the shift's 3 c_x U and 4.5 U^2 terms
+    const T s45 = (T)g_shift.s45, su_ = (T)g_shift.su;
+    auto dsh = [&](T D) { return SHIFT ? D - s45 : D; };
+    auto rsh = [&](T r) { return SHIFT ? r - su_ : r; };
     const T w0 = (T)wd0, w1 = (T)wd1, w2 = (T)wd7;
     const T w1x3 = (T)(3.0 * wd1), w2x3 = (T)(3.0 * wd7);
     v[0] = w0 * B;
@@ -163,25 +185,25 @@ void collide_fast(T (&v)[Q], int x, int nx, T tau, T csmag, T& oux, T& ouy, T& o
         v[i] = fmaT(w, D, E);
         v[i + 1] = fmaT(w, D, -E);
     };
-    pair(1, w1, w1x3, fmaT((T)4.5 * rux, ux, bxx), rux);
+    pair(1, w1, w1x3, dsh(fmaT((T)4.5 * rux, ux, bxx)), rsh(rux));
     pair(3, w1, w1x3, fmaT((T)4.5 * ruy, uy, byy), ruy);
     pair(5, w1, w1x3, fmaT((T)4.5 * ruz, uz, B + azz), ruz);
     const T pxy = bxx + ayy, pxz = bxx + azz, pyz = byy + azz;
     {
         const T su = ux + uy, rs = rux + ruy;
-        pair(7, w2, w2x3, fmaT((T)4.5 * rs, su, pxy + axy), rs);
+        pair(7, w2, w2x3, dsh(fmaT((T)4.5 * rs, su, pxy + axy)), rsh(rs));
     }
     {
         const T su = ux - uy, rs = rux - ruy;
-        pair(9, w2, w2x3, fmaT((T)4.5 * rs, su, pxy - axy), rs);
+        pair(9, w2, w2x3, dsh(fmaT((T)4.5 * rs, su, pxy - axy)), rsh(rs));
     }
     {
         const T su = ux + uz, rs = rux + ruz;
-        pair(11, w2, w2x3, fmaT((T)4.5 * rs, su, pxz + axz), rs);
+        pair(11, w2, w2x3, dsh(fmaT((T)4.5 * rs, su, pxz + axz)), rsh(rs));
     }
     {
         const T su = ux - uz, rs = rux - ruz;
-        pair(13, w2, w2x3, fmaT((T)4.5 * rs, su, pxz - axz), rs);
+        pair(13, w2, w2x3, dsh(fmaT((T)4.5 * rs, su, pxz - axz)), rsh(rs));
     }
     {
         const T su = uy + uz, rs = ruy + ruz;
@@ -271,7 +293,8 @@ void step_cell(const StepArgs<St>& a, int64_t idx, int x, int y, int z, const ty
             if (t == 0) {
                 v[i] = ldv<St>(a.fin, n, i, s);
             } else {
-                v[i] = ldv<St>(a.fin, n, OPP[i], idx);  // w_opp = w_i: deviations carry over
+                v[i] = ldv<St>(a.fin, n, OPP[i], idx);
+                if constexpr (St::shifted) v[i] = v[i] + (T)g_shift.bb[i];  // deviation: + e_opp - e_i
                 if (CX[i] != 0 && t == 2) v[i] = v[i] + K.belt[i] * a.uin;
             }
         }
@@ -423,7 +446,7 @@ void force_impl(const typename St::Store* f, const uint8_t* solid, int nx, int n
                     int64_t s = (x + CX[i]) + (int64_t)nx * ((y + CY[i]) + (int64_t)ny * (z + CZ[i]));
                     if (solid[s] != 1) continue;
                     T v;
-                    if constexpr (St::shifted) v = (T)2.0 * (T)f[(int64_t)i * n + idx];
+                    if constexpr (St::shifted) v = (T)2.0 * ((T)f[(int64_t)i * n + idx] + (T)g_shift.dw[i]);
                     else v = (T)2.0 * (ld<St>(f, n, i, idx, K) - K.w[i]);
                     if (CX[i]) fx = CX[i] > 0 ? fx + v : fx - v;
                     if (CY[i]) fy = CY[i] > 0 ? fy + v : fy - v;
@@ -457,7 +480,7 @@ double mass_impl(const typename St::Store* f, const uint8_t* solid, int64_t n) {
         double c = 0;
         for (int i = 0; i < Q; ++i) {
             double v = (double)f[(int64_t)i * n + idx];
-            if constexpr (St::shifted) v += w_d(i);
+            if constexpr (St::shifted) v += (double)g_shift.e[i];
             c += v;
         }
         tot += c;
@@ -735,5 +758,22 @@ int oracle_cp_f32(const float* mac, const uint8_t* solid, const float* verts, co
 }
 
 uint32_t oracle_rng_hash(uint32_t v) { return pcg_hash(v); }
+
+void oracle_set_shift(double U) {
+    double e[Q];
+    for (int i = 0; i < Q; ++i) {
+        const double cu = 3.0 * CX[i] * U;
+        e[i] = w_d(i) * (1.0 + cu + 0.5 * cu * cu - 1.5 * U * U);
+    }
+    for (int i = 0; i < Q; ++i) {
+        g_shift.e[i] = (float)(U != 0.0 ? e[i] : w_d(i));
+        g_shift.bb[i] = (float)(e[OPP[i]] - e[i]);
+        g_shift.dw[i] = (float)(e[i] - w_d(i));
+    }
+    g_shift.su = (float)U;
+    g_shift.suu = (float)(U * U);
+    g_shift.s45 = (float)(4.5 * U * U);
+    g_shift.s15 = (float)(1.5 * U * U);
+}
 
 }  // extern "C"

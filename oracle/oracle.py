@@ -50,6 +50,8 @@ def lib():
         L.oracle_cp_f32.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32, i64, f32, f32]
         L.oracle_rng_hash.argtypes = [ctypes.c_uint32]
         L.oracle_rng_hash.restype = ctypes.c_uint32
+        L.oracle_set_shift.argtypes = [f64]
+        L.oracle_set_shift.restype = None
         _lib = L
     return _lib
 
@@ -77,11 +79,26 @@ def _chk(rc, what):
         raise RuntimeError(f'oracle {what} failed: {rc}')
 
 
+def shift_values(U):
+    """float32 shifts e_i of half-width storage: w_i (1 + 3 c_xi U + 4.5 c_xi^2 U^2 - 1.5 U^2)
+    in double, rounded once (oracle_set_shift); U = 0 gives the rest weights."""
+    if U == 0.0:
+        return W.astype(np.float32)
+    cx = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0], np.float64)
+    out = []
+    for i in range(Q):
+        cu = 3.0 * cx[i] * U
+        out.append(W[i] * (1.0 + cu + 0.5 * cu * cu - 1.5 * U * U))
+    return np.array(out, np.float32)
+
+
 class Lattice:
     """The reference Solver's device state held in host numpy arrays (server/lbm.py:398-413)."""
 
-    def __init__(self, dims, prec=F32, collision=0):
+    def __init__(self, dims, prec=F32, collision=0, shift_u=0.0):
         self.collision = int(collision)  # 0 reference order, 1 moment-space form
+        # fp16/bf16 storage shift velocity (the library's wt_grid.shift_u; 0 = rest weights)
+        self.shift_u = float(shift_u)
         self.nx, self.ny, self.nz = (int(d) for d in dims)
         self.n = n = self.nx * self.ny * self.nz
         self.prec = prec
@@ -91,12 +108,17 @@ class Lattice:
         self.mac = np.zeros((n, 4), rd)
         self.cur = 0
 
+    def _shift(self):
+        lib().oracle_set_shift(self.shift_u)
+
     def reset(self, uin):
+        self._shift()
         for buf in self.f:
             _chk(lib().oracle_init(self.prec, _p(buf), _p(self.mac), self.n, float(uin)), 'init')
 
     def step(self, steps, uin, tau, smag, serial=False):
         L = lib()
+        self._shift()
         for _ in range(int(steps)):
             _chk(L.oracle_step(self.prec, _p(self.f[self.cur]), _p(self.f[1 - self.cur]), _p(self.solid),
                                _p(self.mac), self.nx, self.ny, self.nz, float(uin), float(tau), float(smag),
@@ -109,22 +131,25 @@ class Lattice:
         ref = np.zeros(3, rd)
         d = np.zeros(3, np.float64)
         b = np.zeros(3, np.float64)
+        self._shift()
         _chk(lib().oracle_force(self.prec, _p(self.f[self.cur]), _p(self.solid), self.nx, self.ny, self.nz,
                                 _p(ref), _p(d), _p(b)), 'force')
         return ref, d, b
 
     def mass(self):
         out = np.zeros(1, np.float64)
+        self._shift()
         _chk(lib().oracle_mass(self.prec, _p(self.f[self.cur]), _p(self.solid), self.n, _p(out)), 'mass')
         return float(out[0])
 
     def populations(self, which=None):
         """Populations of buffer ``which`` (default: current) as float64, unshifted, shape (19, n)."""
         buf = self.f[self.cur if which is None else which]
+        e = shift_values(self.shift_u).astype(np.float64)[:, None]
         if self.prec == F16:
-            v = buf.astype(np.float64).reshape(Q, self.n) + W[:, None]
+            v = buf.astype(np.float64).reshape(Q, self.n) + e
         elif self.prec == BF16:
-            v = (buf.astype(np.uint32) << 16).view(np.float32).astype(np.float64).reshape(Q, self.n) + W[:, None]
+            v = (buf.astype(np.uint32) << 16).view(np.float32).astype(np.float64).reshape(Q, self.n) + e
         else:
             v = buf.astype(np.float64).reshape(Q, self.n)
         return v

@@ -37,7 +37,7 @@ def test_exports_every_declared_symbol(L):
 
 
 def test_abi_version(L):
-    assert L.wt_abi_version() == 1
+    assert L.wt_abi_version() == W.ABI_VERSION == 2
 
 
 @pytest.mark.parametrize('dims,ok', [((128, 64, 64), True), ((4, 3, 3), True), ((12, 8, 10), True),
@@ -64,7 +64,7 @@ def test_null_arguments_rejected_before_any_launch(L):
     assert b'null' in L.wt_last_error()
     g = W.Grid(16, 8, 8, W.F32)
     assert L.wt_step(ctypes.byref(g), 0, 1, 0.05, 0.5, 0.1, 1, None) == W.WT_ERR_ARG
-    assert L.wt_init_eq(W.F32, None, None, 10, 0.05, None) == W.WT_ERR_ARG
+    assert L.wt_init_eq(W.F32, None, None, 10, 0.05, 0.0, None) == W.WT_ERR_ARG
     assert L.wt_forces(None, 0, None, None, 0, None, None, None) == W.WT_ERR_ARG
     assert L.wt_mass(None, 0, None, None, None) == W.WT_ERR_ARG
     assert L.wt_slice(None, None, None, 16, 8, 8, 0, 0, 0, 0.05, 1.0, 0.0, 1.0, None) == W.WT_ERR_ARG
@@ -78,7 +78,7 @@ def test_bad_enums_rejected(L):
     assert b'precision' in L.wt_last_error()
     g.precision = W.F32
     assert L.wt_step(ctypes.byref(g), 2, 1, 0.05, 0.5, 0.1, 1, None) == W.WT_ERR_ARG
-    assert L.wt_init_eq(9, fake, fake, 10, 0.05, None) == W.WT_ERR_ARG
+    assert L.wt_init_eq(9, fake, fake, 10, 0.05, 0.0, None) == W.WT_ERR_ARG
     g.nx = 15
     assert L.wt_step(ctypes.byref(g), 0, 1, 0.05, 0.5, 0.1, 1, None) == W.WT_ERR_DIMS
     g.nx = 16

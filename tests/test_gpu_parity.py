@@ -140,15 +140,20 @@ def _random_case(dims, seed, belt=True):
     return solid
 
 
-@pytest.mark.parametrize('prec_name,oprec', [('fp32', 0), ('fp16', 1), ('bf16', 2), ('fp64', 3)])
+@pytest.mark.parametrize('prec_name,oprec,shift', [('fp32', 0, 'free-stream'), ('fp16', 1, 'free-stream'),
+                                                    ('bf16', 2, 'free-stream'), ('fp16', 1, 'rest'),
+                                                    ('bf16', 2, 'rest'), ('fp64', 3, 'free-stream')])
 @pytest.mark.parametrize('dims', [(64, 24, 20), (34, 9, 7)])
-def test_random_obstacles_match_oracle(oracle_mod, prec_name, oprec, dims):
-    """Larger grids than the goldens, every storage precision, against the pinned oracle."""
+def test_random_obstacles_match_oracle(oracle_mod, prec_name, oprec, shift, dims):
+    """Larger grids than the goldens, every storage precision (half-width storage shifted by
+    the free-stream equilibrium and by the rest weights), against the pinned oracle."""
     solid = _random_case(dims, 5)
     uin, tau, smag = 0.06, 0.52, 0.16
-    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name)
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name, shift=shift)
     s.reset(uin)
-    L = oracle_mod.Lattice(dims, oprec)
+    if oprec in (1, 2):
+        assert float(s.grid.shift_u) == (float(np.float32(uin)) if shift == 'free-stream' else 0.0)
+    L = oracle_mod.Lattice(dims, oprec, shift_u=float(s.grid.shift_u))
     L.solid[:] = solid
     L.reset(uin)
     p = dict(uIn=uin, tau=tau, smag=smag)
@@ -216,11 +221,12 @@ def test_every_tile_variant_matches_oracle(oracle_mod, prec_name, oprec):
     dims = (64, 20, 12)
     solid = _random_case(dims, 17)
     uin, tau, smag = 0.05, 0.51, 0.16
-    L = oracle_mod.Lattice(dims, oprec)
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name)
+    s.reset(uin)
+    L = oracle_mod.Lattice(dims, oprec, shift_u=float(s.grid.shift_u))
     L.solid[:] = solid
     L.reset(uin)
     L.step(5, uin, tau, smag)
-    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name)
     tiles = autotune.admissible(s)
     assert len(tiles) >= 4
     for tile in tiles:
@@ -258,12 +264,13 @@ def test_fast_collision_matches_oracle(oracle_mod, prec_name, oprec, dims):
     import autotune
     solid = _random_case(dims, 23)
     uin, tau, smag = 0.07, 0.515, 0.16
-    L = oracle_mod.Lattice(dims, oprec, collision=1)
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name, collision='fast')
+    s.reset(uin)
+    L = oracle_mod.Lattice(dims, oprec, collision=1, shift_u=float(s.grid.shift_u))
     L.solid[:] = solid
     L.reset(uin)
     L.step(5, uin, tau, smag)
     ref = L.populations()
-    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name, collision='fast')
     p = dict(uIn=uin, tau=tau, smag=smag)
     tiles = autotune.admissible(s)
     assert tiles
@@ -288,8 +295,9 @@ def _random_flow(s, seed, umax=0.3):
     rho = rng.uniform(0.95, 1.05, s.n)
     cu = u @ c.T
     f = (w[None, :] * rho[:, None] * (1 + 3 * cu + 4.5 * cu * cu - 1.5 * (u * u).sum(1)[:, None])).T
-    if s.precision in (1, 2):  # shifted storage
-        f = f - w[:, None]
+    if s.precision in (1, 2):  # shifted storage holds f - e
+        from lbm import shift_values
+        f = f - shift_values(float(s.grid.shift_u)).astype(np.float64)[:, None]
     _load(s, s.cur, f.reshape(-1))
 
 

@@ -205,6 +205,7 @@ void fill_desc(const wt_grid& g, int32_t cur0, double uin, double tau, double sm
     a.mac_all = mac_all;
     a.status = g.status;
     a.test_skip_chunk = 0;
+    set_shift(a, Prec<PREC>::shifted ? (double)g.shift_u : 0.0);
     std::memcpy(out, &a, sizeof(a));
 }
 

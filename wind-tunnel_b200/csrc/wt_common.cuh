@@ -60,18 +60,51 @@ template <> struct Prec<WT_F64> {
     __device__ static __forceinline__ S from(double v) { return v; }
 };
 
-// population value as the collision sees it
+// population value as the collision sees it; shifted storage holds f - e (e: the shift of
+// population I, see ShiftTables)
 template <class P, int I>
-__device__ __forceinline__ typename P::T ld_pop(const typename P::S* p) {
-    using T = typename P::T;
-    if constexpr (P::shifted) return P::to(*p) + (T)wd(I);
+__device__ __forceinline__ typename P::T ld_pop(const typename P::S* p, typename P::T e) {
+    if constexpr (P::shifted) return P::to(*p) + e;
     else return P::to(*p);
 }
 template <class P, int I>
-__device__ __forceinline__ void st_pop(typename P::S* p, typename P::T v) {
-    using T = typename P::T;
-    if constexpr (P::shifted) *p = P::from(v - (T)wd(I));
+__device__ __forceinline__ void st_pop(typename P::S* p, typename P::T v, typename P::T e) {
+    if constexpr (P::shifted) *p = P::from(v - e);
     else *p = P::from(v);
+}
+
+// Shift of half-width (fp16/bf16) population storage: populations are stored as
+// d_i = f_i - e_i with e_i the equilibrium at rho = 1, u = (U, 0, 0) (wt_grid.shift_u). Near
+// the free stream the stored deviations are then small, which is where half precision has
+// its absolute resolution. U = 0 gives e_i = w_i, the rest weights. All tables are evaluated
+// in double and rounded once:
+//   e_i  = w_i (1 + 3 cx_i U + 4.5 cx_i^2 U^2 - 1.5 U^2)
+//   bb_i = e_opp(i) - e_i          (bounce-back in deviation form)
+//   dw_i = e_i - w_i               (momentum exchange uses f_i - w_i)
+//   su = U, suu = U^2, s45 = 4.5 U^2, s15 = 1.5 U^2 (moment-space collision)
+struct ShiftTables {
+    bool on;  // U != 0
+    double e[Q], bb[Q], dw[Q];
+    double su, suu, s45, s15;
+};
+inline ShiftTables shift_tables(double U) {
+    ShiftTables t;
+    t.on = U != 0.0;
+    double e[Q];
+    for (int i = 0; i < Q; ++i) {
+        const double cu = 3.0 * cx(i) * U;
+        e[i] = wd(i) * (1.0 + cu + 0.5 * cu * cu - 1.5 * U * U);
+    }
+    for (int i = 0; i < Q; ++i) {
+        t.e[i] = t.on ? e[i] : wd(i);
+        t.bb[i] = e[opp(i)] - e[i];
+        t.dw[i] = e[i] - wd(i);
+    }
+    t.su = U;
+    t.suu = U * U;
+    t.s45 = 4.5 * U * U;
+    t.s15 = 1.5 * U * U;
+    return t;
 }
 
 // Division of non-negative 32-bit ints below 2^31 by a fixed divisor via multiply-high

@@ -39,12 +39,19 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* __re
     }
 }
 
+// per-population constants of the shifted storage passed by value
+template <class T>
+struct PopVals {
+    T v[Q];
+};
+
 template <int PREC>
 __global__ void __launch_bounds__(RED_THREADS) k_force_partial(const typename Prec<PREC>::S* __restrict__ f,
                                                                const int32_t* __restrict__ cells,
                                                                const uint32_t* __restrict__ masks, int64_t count,
                                                                int64_t n, int32_t nx, int32_t nxy, FastDiv dnx,
-                                                               FastDiv dnxy, double* __restrict__ partials) {
+                                                               FastDiv dnxy, PopVals<typename Prec<PREC>::T> dw,
+                                                               double* __restrict__ partials) {
     using P = Prec<PREC>;
     using T = typename P::T;
     double acc[FORCE_VALS] = {0, 0, 0, 0, 0, 0};
@@ -57,9 +64,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_force_partial(const typename Pr
         unroll<1, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             if (m & (1u << (i - 1))) {
-                // 2 (f_i - w_i) per link (server/lbm.py:189); shifted storage holds f_i - w_i
+                // 2 (f_i - w_i) per link (server/lbm.py:189); shifted storage holds f_i - e_i,
+                // so f_i - w_i = stored + (e_i - w_i)
                 T v;
-                if constexpr (P::shifted) v = (T)2.0 * P::to(f[(int64_t)i * n + idx]);
+                if constexpr (P::shifted) v = (T)2.0 * (P::to(f[(int64_t)i * n + idx]) + dw.v[i]);
                 else v = (T)2.0 * (P::to(f[(int64_t)i * n + idx]) - (T)wd(i));
                 if constexpr (cx(i) > 0) fx = fx + v;
                 if constexpr (cx(i) < 0) fx = fx - v;
@@ -99,6 +107,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_final(const double* __restrict_
 template <int PREC>
 __global__ void __launch_bounds__(RED_THREADS) k_mass_partial(const typename Prec<PREC>::S* __restrict__ f,
                                                               const uint8_t* __restrict__ solid, int64_t n,
+                                                              PopVals<typename Prec<PREC>::T> e,
                                                               double* __restrict__ partials) {
     using P = Prec<PREC>;
     double acc[1] = {0.0};
@@ -108,12 +117,21 @@ __global__ void __launch_bounds__(RED_THREADS) k_mass_partial(const typename Pre
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             double v = (double)P::to(f[(int64_t)i * n + idx]);
-            if constexpr (P::shifted) v += wd(i);
+            if constexpr (P::shifted) v += (double)e.v[i];  // the shift as the kernels apply it
             c += v;
         });
         acc[0] += c;
     }
     block_reduce_store<1>(acc, partials + blockIdx.x);
+}
+
+template <int PREC>
+PopVals<typename Prec<PREC>::T> shift_vals(const wt_grid* g, bool dw) {
+    using T = typename Prec<PREC>::T;
+    const ShiftTables t = shift_tables(Prec<PREC>::shifted ? (double)g->shift_u : 0.0);
+    PopVals<T> r;
+    for (int i = 0; i < Q; ++i) r.v[i] = (T)(dw ? t.dw[i] : t.e[i]);
+    return r;
 }
 
 template <int PREC>
@@ -124,7 +142,8 @@ int forces_impl(const wt_grid* g, int32_t cur, const int32_t* cells, const uint3
     const int64_t n = (int64_t)nxy * g->nz;
     k_force_partial<PREC><<<RED_BLOCKS, RED_THREADS, 0, st>>>(static_cast<const S*>(g->f[cur]), cells, masks, count,
                                                               n, g->nx, nxy, FastDiv((uint32_t)g->nx),
-                                                              FastDiv((uint32_t)nxy), partials);
+                                                              FastDiv((uint32_t)nxy), shift_vals<PREC>(g, true),
+                                                              partials);
     k_final<FORCE_VALS><<<1, RED_THREADS, 0, st>>>(partials, RED_BLOCKS, out6);
     return wt_cuda_check("wt_forces launch");
 }
@@ -133,7 +152,8 @@ template <int PREC>
 int mass_impl(const wt_grid* g, int32_t cur, double* partials, double* out1, cudaStream_t st) {
     using S = typename Prec<PREC>::S;
     const int64_t n = (int64_t)g->nx * g->ny * g->nz;
-    k_mass_partial<PREC><<<RED_BLOCKS, RED_THREADS, 0, st>>>(static_cast<const S*>(g->f[cur]), g->solid, n, partials);
+    k_mass_partial<PREC><<<RED_BLOCKS, RED_THREADS, 0, st>>>(static_cast<const S*>(g->f[cur]), g->solid, n,
+                                                             shift_vals<PREC>(g, false), partials);
     k_final<1><<<1, RED_THREADS, 0, st>>>(partials, RED_BLOCKS, out1);
     return wt_cuda_check("wt_mass launch");
 }
@@ -228,7 +248,7 @@ static int forces_noalloc_impl(const wt_grid* g, int32_t cur, const int32_t* cel
     if (nb > 0)
         k_force_partial<PREC><<<nb, RED_THREADS, 0, st>>>(static_cast<const S*>(g->f[cur]), cells, masks, count, n,
                                                            g->nx, nxy, FastDiv((uint32_t)g->nx), FastDiv((uint32_t)nxy),
-                                                           partials);
+                                                           shift_vals<PREC>(g, true), partials);
     k_final<FORCE_VALS><<<1, RED_THREADS, 0, st>>>(partials, nb, out6);
     return wt_cuda_check("wt_forces_noalloc launch");
 }

@@ -11,7 +11,7 @@ struct InitVals {
 
 template <int PREC>
 __global__ void __launch_bounds__(256) k_init(typename Prec<PREC>::S* __restrict__ f, typename Prec<PREC>::T* __restrict__ mac,
-                                              int64_t n, typename Prec<PREC>::T uin) {
+                                              int64_t n, typename Prec<PREC>::T uin, InitVals<typename Prec<PREC>::T> e) {
     using P = Prec<PREC>;
     using T = typename P::T;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x) {
@@ -20,7 +20,7 @@ __global__ void __launch_bounds__(256) k_init(typename Prec<PREC>::S* __restrict
             // W * (1 + 3 c_x u + 4.5 c_x^2 u u - 1.5 u u), left to right as generated (:68)
             const T v = (T)wd(i) * ((T)1.0 + (T)(3.0 * cx(i)) * uin + (T)(4.5 * cx(i) * cx(i)) * uin * uin -
                                     (T)1.5 * uin * uin);
-            st_pop<P, i>(f + i * n + idx, v);
+            st_pop<P, i>(f + i * n + idx, v, e.v[i]);
         });
         mac[4 * idx + 0] = uin;
         mac[4 * idx + 1] = (T)0.0;
@@ -175,11 +175,14 @@ __global__ void __launch_bounds__(LINK_THREADS) k_links_fill(const uint8_t* __re
 }
 
 template <int PREC>
-int init_impl(void* f, void* mac, int64_t n, double uin, cudaStream_t st) {
+int init_impl(void* f, void* mac, int64_t n, double uin, double shift_u, cudaStream_t st) {
     using P = Prec<PREC>;
     using T = typename P::T;
+    const ShiftTables t = shift_tables(P::shifted ? shift_u : 0.0);
+    InitVals<T> e;
+    for (int i = 0; i < Q; ++i) e.v[i] = (T)t.e[i];
     const int64_t nb = std::min<int64_t>((n + 255) / 256, 148 * 64);
-    k_init<PREC><<<(unsigned)nb, 256, 0, st>>>(static_cast<typename P::S*>(f), static_cast<T*>(mac), n, (T)uin);
+    k_init<PREC><<<(unsigned)nb, 256, 0, st>>>(static_cast<typename P::S*>(f), static_cast<T*>(mac), n, (T)uin, e);
     return wt_cuda_check("wt_init_eq launch");
 }
 
@@ -187,14 +190,15 @@ int init_impl(void* f, void* mac, int64_t n, double uin, cudaStream_t st) {
 
 using namespace wt;
 
-extern "C" int wt_init_eq(int32_t precision, void* f, void* mac, int64_t n, double uin, void* stream) {
+extern "C" int wt_init_eq(int32_t precision, void* f, void* mac, int64_t n, double uin, double shift_u,
+                          void* stream) {
     if (!f || !mac || n <= 0) return wt_set_error(WT_ERR_ARG, "wt_init_eq: null buffer or n <= 0");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch (precision) {
-        case WT_F32: return init_impl<WT_F32>(f, mac, n, uin, st);
-        case WT_F16: return init_impl<WT_F16>(f, mac, n, uin, st);
-        case WT_BF16: return init_impl<WT_BF16>(f, mac, n, uin, st);
-        case WT_F64: return init_impl<WT_F64>(f, mac, n, uin, st);
+        case WT_F32: return init_impl<WT_F32>(f, mac, n, uin, shift_u, st);
+        case WT_F16: return init_impl<WT_F16>(f, mac, n, uin, shift_u, st);
+        case WT_BF16: return init_impl<WT_BF16>(f, mac, n, uin, shift_u, st);
+        case WT_F64: return init_impl<WT_F64>(f, mac, n, uin, shift_u, st);
         default: return wt_set_error(WT_ERR_ARG, "wt_init_eq: unknown precision %d", precision);
     }
 }

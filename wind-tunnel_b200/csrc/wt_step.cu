@@ -115,6 +115,7 @@ int step_impl(const wt_grid* g, int32_t cur, int32_t steps, double uin, double t
         return wt_set_error(WT_ERR_ARG, "wt_step: code buffer not 16-byte aligned");
     a.status = g->status;
     a.test_skip_chunk = g->test_skip_chunk;
+    set_shift(a, P::shifted ? (double)g->shift_u : 0.0);
     constexpr int VEC = 16 / (int)sizeof(S);
     const int32_t nface = a.nxy + a.nx * (a.nz - 2);
     const unsigned nb_face = (unsigned)((nface + 255) / 256);

@@ -57,6 +57,25 @@ struct StepArgs {
     int32_t chunk_r[Q];
     int32_t* status;           // device word for bounded-wait failures (may be null)
     int32_t test_skip_chunk;   // test hook: when > 0, chunk test_skip_chunk-1 is never loaded
+    // shifted storage (ShiftTables of wt_grid.shift_u, rounded to T)
+    T e[Q], bb[Q];
+    T su, suu, s45, s15;
+};
+
+template <class S, class T>
+inline void set_shift(StepArgs<S, T>& a, double shift_u) {
+    const ShiftTables t = shift_tables(shift_u);
+    for (int i = 0; i < Q; ++i) {
+        a.e[i] = (T)t.e[i];
+        a.bb[i] = (T)t.bb[i];
+    }
+    a.su = (T)t.su; a.suu = (T)t.suu; a.s45 = (T)t.s45; a.s15 = (T)t.s15;
+}
+
+// the shift constants the moment-space collision needs (a pair: broadcast to both lanes)
+template <class T>
+struct ShiftK {
+    T su, suu, s45, s15;
 };
 
 template <class T>
@@ -150,7 +169,7 @@ __device__ __forceinline__ void face_eq(const StepArgs<typename P::S, typename P
         if constexpr (cz(i) > 0) s = s + buz;
         if constexpr (cz(i) < 0) s = s - buz;
         const T bc = (T)3.0 * s;
-        st_pop<P, i>(a.dst[i] + idx, (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq));
+        st_pop<P, i>(a.dst[i] + idx, (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq), a.e[i]);
     });
 }
 
@@ -369,24 +388,26 @@ __device__ __forceinline__ F2 xcoord<F2>(int32_t x) { return F2((float)x, (float
 // lane at a time: compiled on F2 inside the full collision, this one expression came out a
 // last-bit different from the one-cell form in about 0.5% of cells (though its F2 form alone
 // matches), and per-lane evaluation restores identical bits at a cost of a few instructions.
+// With SHIFT the outputs are deviations from the shift e_i, so B also carries + 1.5 U^2.
 template <class T, bool SHIFT>
 struct BTerm {
-    __device__ static __forceinline__ T eval(T rho, T S, T usq, T axx, T ayy, T azz) {
+    __device__ static __forceinline__ T eval(T rho, T S, T usq, T axx, T ayy, T azz, T s15) {
         const T tra3 = ((axx + ayy) + azz) * (T)(1.0 / 3.0);
-        return fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+        const T b = fmaT(-rho, (T)1.5 * usq, SHIFT ? S : rho) - tra3;
+        return SHIFT ? b + s15 : b;
     }
 };
 template <bool SHIFT>
 struct BTerm<F2, SHIFT> {
-    __device__ static __forceinline__ F2 eval(F2 rho, F2 S, F2 usq, F2 axx, F2 ayy, F2 azz) {
-        return F2(BTerm<float, SHIFT>::eval(rho.v.x, S.v.x, usq.v.x, axx.v.x, ayy.v.x, azz.v.x),
-                  BTerm<float, SHIFT>::eval(rho.v.y, S.v.y, usq.v.y, axx.v.y, ayy.v.y, azz.v.y));
+    __device__ static __forceinline__ F2 eval(F2 rho, F2 S, F2 usq, F2 axx, F2 ayy, F2 azz, F2 s15) {
+        return F2(BTerm<float, SHIFT>::eval(rho.v.x, S.v.x, usq.v.x, axx.v.x, ayy.v.x, azz.v.x, s15.v.x),
+                  BTerm<float, SHIFT>::eval(rho.v.y, S.v.y, usq.v.y, axx.v.y, ayy.v.y, azz.v.y, s15.v.y));
     }
 };
 
 template <class T, bool SHIFT>
-__device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T tau, T csmag, T& oux, T& ouy,
-                                             T& ouz, T& orho) {
+__device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T tau, T csmag, const ShiftK<T>& sk,
+                                             T& oux, T& ouy, T& ouz, T& orho) {
     const T s1 = v[1] + v[2], a1 = v[1] - v[2];
     const T s3 = v[3] + v[4], a3 = v[3] - v[4];
     const T s5 = v[5] + v[6], a5 = v[5] - v[6];
@@ -397,10 +418,13 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
     const T s15 = v[15] + v[16], a15 = v[15] - v[16];
     const T s17 = v[17] + v[18], a17 = v[17] - v[18];
     const T d7 = s7 + s9, d11 = s11 + s13, d15 = s15 + s17;
-    const T xxx = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
+    // with SHIFT: + U^2 in xx and + U in jx restore the moments of the shift e_i
+    const T xxx0 = (s1 + d7) + d11, xyy = (s3 + d7) + d15, xzz = (s5 + d11) + d15;
+    const T xxx = SHIFT ? xxx0 + sk.suu : xxx0;
     const T xxy = s7 - s9, xxz = s11 - s13, xyz = s15 - s17;
     const T S = ((v[0] + s1) + (s3 + s5)) + ((d7 + d11) + d15);
-    const T jx = ((a1 + a7) + (a9 + a11)) + a13;
+    const T jx0 = ((a1 + a7) + (a9 + a11)) + a13;
+    const T jx = SHIFT ? jx0 + sk.su : jx0;
     const T jy = ((a3 + a7) - (a9 - a15)) + a17;
     const T jz = ((a5 + a11) - (a13 - a15)) - a17;
     const T rho = SHIFT ? S + (T)1.0 : S;
@@ -427,13 +451,16 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
     const T k45 = (T)4.5 * keep, k9 = (T)9.0 * keep;
     const T axx = k45 * nxx, ayy = k45 * nyy, azz = k45 * nzz;
     const T axy = k9 * nxy, axz = k9 * nxz, ayz = k9 * nyz;  // 2 A_ab
-    const T B = BTerm<T, SHIFT>::eval(rho, S, usq, axx, ayy, azz);
+    const T B = BTerm<T, SHIFT>::eval(rho, S, usq, axx, ayy, azz, sk.s15);
+    // with SHIFT, a direction with c_x != 0 drops 3 c_x U from its odd term and 4.5 U^2 from
+    // its even term (the shift's own terms): rux/rs less su, D less s45
     const T w0 = (T)wd(0), w1 = (T)wd(1), w2 = (T)wd(7);
     const T w1x3 = (T)(3.0 * wd(1)), w2x3 = (T)(3.0 * wd(7));
     v[0] = w0 * B;
     const T bxx = B + axx, byy = B + ayy;
     {
-        const T D = fmaT((T)4.5 * rux, ux, bxx), E = w1x3 * rux;
+        const T D0 = fmaT((T)4.5 * rux, ux, bxx);
+        const T D = SHIFT ? D0 - sk.s45 : D0, E = w1x3 * (SHIFT ? rux - sk.su : rux);
         v[1] = fmaT(w1, D, E); v[2] = fmaT(w1, D, -E);
     }
     {
@@ -447,22 +474,26 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
     const T pxy = bxx + ayy, pxz = bxx + azz, pyz = byy + azz;
     {
         const T su = ux + uy, rs = rux + ruy;
-        const T D = fmaT((T)4.5 * rs, su, pxy + axy), E = w2x3 * rs;
+        const T D0 = fmaT((T)4.5 * rs, su, pxy + axy);
+        const T D = SHIFT ? D0 - sk.s45 : D0, E = w2x3 * (SHIFT ? rs - sk.su : rs);
         v[7] = fmaT(w2, D, E); v[8] = fmaT(w2, D, -E);
     }
     {
         const T su = ux - uy, rs = rux - ruy;
-        const T D = fmaT((T)4.5 * rs, su, pxy - axy), E = w2x3 * rs;
+        const T D0 = fmaT((T)4.5 * rs, su, pxy - axy);
+        const T D = SHIFT ? D0 - sk.s45 : D0, E = w2x3 * (SHIFT ? rs - sk.su : rs);
         v[9] = fmaT(w2, D, E); v[10] = fmaT(w2, D, -E);
     }
     {
         const T su = ux + uz, rs = rux + ruz;
-        const T D = fmaT((T)4.5 * rs, su, pxz + axz), E = w2x3 * rs;
+        const T D0 = fmaT((T)4.5 * rs, su, pxz + axz);
+        const T D = SHIFT ? D0 - sk.s45 : D0, E = w2x3 * (SHIFT ? rs - sk.su : rs);
         v[11] = fmaT(w2, D, E); v[12] = fmaT(w2, D, -E);
     }
     {
         const T su = ux - uz, rs = rux - ruz;
-        const T D = fmaT((T)4.5 * rs, su, pxz - axz), E = w2x3 * rs;
+        const T D0 = fmaT((T)4.5 * rs, su, pxz - axz);
+        const T D = SHIFT ? D0 - sk.s45 : D0, E = w2x3 * (SHIFT ? rs - sk.su : rs);
         v[13] = fmaT(w2, D, E); v[14] = fmaT(w2, D, -E);
     }
     {
@@ -479,26 +510,36 @@ __device__ __forceinline__ void collide_fast(T (&v)[Q], int32_t x, int32_t nx, T
 }
 
 // collision dispatch: FAST selects the moment-space form, on deviations for shifted storage
+template <class S, class T>
+__device__ __forceinline__ ShiftK<T> shiftk(const StepArgs<S, T>& a) {
+    return ShiftK<T>{a.su, a.suu, a.s45, a.s15};
+}
+template <class S, class T>
+__device__ __forceinline__ ShiftK<F2> shiftk2(const StepArgs<S, T>& a) {
+    return ShiftK<F2>{F2(a.su), F2(a.suu), F2(a.s45), F2(a.s15)};
+}
+
 template <class P, bool FAST>
 __device__ __forceinline__ void collide_any(typename P::T (&f)[Q], int32_t x, int32_t nx, typename P::T tau,
-                                            typename P::T csmag, typename P::T& ux, typename P::T& uy,
-                                            typename P::T& uz, typename P::T& rho) {
-    if constexpr (FAST) collide_fast<typename P::T, P::shifted>(f, x, nx, tau, csmag, ux, uy, uz, rho);
+                                            typename P::T csmag, const ShiftK<typename P::T>& sk,
+                                            typename P::T& ux, typename P::T& uy, typename P::T& uz,
+                                            typename P::T& rho) {
+    if constexpr (FAST) collide_fast<typename P::T, P::shifted>(f, x, nx, tau, csmag, sk, ux, uy, uz, rho);
     else collide<typename P::T>(f, x, nx, tau, csmag, ux, uy, uz, rho);
 }
 
 // population value as the collision of mode FAST takes it: f_i (+ w_i undone for shifted
 // storage in the exact form), or the stored deviation itself in the fast form
-template <class P, bool FAST, int I>
-__device__ __forceinline__ typename P::T ld_in(const typename P::S* p) {
+template <class P, bool FAST, int I, class A>
+__device__ __forceinline__ typename P::T ld_in(const A& a, const typename P::S* p) {
     if constexpr (FAST) return P::to(*p);
-    else return ld_pop<P, I>(p);
+    else return ld_pop<P, I>(p, a.e[I]);
 }
 
-template <class P, bool FAST, int I>
-__device__ __forceinline__ void st_out(typename P::S* p, typename P::T v) {
+template <class P, bool FAST, int I, class A>
+__device__ __forceinline__ void st_out(const A& a, typename P::S* p, typename P::T v) {
     if constexpr (FAST) *p = P::from(v);
-    else st_pop<P, I>(p, v);
+    else st_pop<P, I>(p, v, a.e[I]);
 }
 
 // Pull of one cell with bounce-back and moving belt where a source is non-fluid
@@ -507,19 +548,20 @@ template <class P, bool FAST>
 __device__ __forceinline__ void pull_generic(const StepArgs<typename P::S, typename P::T>& a, int32_t idx,
                                              bool near, typename P::T (&f)[Q]) {
     using T = typename P::T;
-    f[0] = ld_in<P, FAST, 0>(a.src[0] + idx);
+    f[0] = ld_in<P, FAST, 0>(a, a.src[0] + idx);
     unroll<1, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         if (!near) {
-            f[i] = ld_in<P, FAST, i>(a.src[i] + idx);
+            f[i] = ld_in<P, FAST, i>(a, a.src[i] + idx);
         } else {
             const int32_t off = cx(i) + cy(i) * a.nx + cz(i) * a.nxy;
             const int t = a.solid[idx - off];
             if (t == 0) {
-                f[i] = ld_in<P, FAST, i>(a.src[i] + idx);
+                f[i] = ld_in<P, FAST, i>(a, a.src[i] + idx);
             } else {
-                // bounce-back; in deviation form w_opp(i) = w_i, so the value carries over
-                f[i] = ld_in<P, FAST, opp(i)>(a.fin + (int64_t)opp(i) * a.n + idx);
+                // bounce-back; in deviation form the shift difference e_opp(i) - e_i is added
+                f[i] = ld_in<P, FAST, opp(i)>(a, a.fin + (int64_t)opp(i) * a.n + idx);
+                if constexpr (FAST && P::shifted) f[i] = f[i] + a.bb[i];
                 if constexpr (cx(i) != 0) {
                     if (t == 2) f[i] = f[i] + (T)(6.0 * wd(i) * cx(i)) * a.uin;
                 }
@@ -533,7 +575,7 @@ __device__ __forceinline__ void store_cell(const StepArgs<typename P::S, typenam
                                            const typename P::T (&f)[Q]) {
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        st_out<P, FAST, i>(a.dst[i] + idx, f[i]);
+        st_out<P, FAST, i>(a, a.dst[i] + idx, f[i]);
     });
 }
 
@@ -567,7 +609,7 @@ __device__ __forceinline__ void general_cell(const StepArgs<typename P::S, typen
     } else {
         T f[Q];
         pull_generic<P, FAST>(a, idx, (code & CODE_NEAR) != 0, f);
-        collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, mx, my, mz, mr);
+        collide_any<P, FAST>(f, x, nx, a.tau, a.csmag, shiftk(a), mx, my, mz, mr);
         store_cell<P, FAST>(a, idx, f);
         write = write || row_shell || x == 1 || x == nx - 2;
     }
@@ -612,7 +654,7 @@ __device__ __forceinline__ void collide_cells(const StepArgs<typename P::S, type
 #pragma unroll
             for (int i = 0; i < Q; ++i) g[i] = F2(f[k][i], f[k + 1][i]);
             F2 ux, uy, uz, rho;
-            collide_fast<F2, P::shifted>(g, x0 + k, nx, F2(a.tau), F2(a.csmag), ux, uy, uz, rho);
+            collide_fast<F2, P::shifted>(g, x0 + k, nx, F2(a.tau), F2(a.csmag), shiftk2(a), ux, uy, uz, rho);
 #pragma unroll
             for (int i = 0; i < Q; ++i) {
                 f[k][i] = g[i].v.x;
@@ -627,7 +669,7 @@ __device__ __forceinline__ void collide_cells(const StepArgs<typename P::S, type
     } else {
 #pragma unroll
         for (int k = 0; k < V; ++k) {
-            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, mx, my, mz, mr);
+            collide_any<P, FAST>(f[k], x0 + k, nx, a.tau, a.csmag, shiftk(a), mx, my, mz, mr);
             if (a.mac_all || row_shell || x0 + k == 1 || x0 + k == nx - 2) store_mac(a.mac_cur, idx0 + k, mx, my, mz, mr);
         }
     }
@@ -635,9 +677,9 @@ __device__ __forceinline__ void collide_cells(const StepArgs<typename P::S, type
 
 // Face equilibrium populations from (br, bux, buy, buz), the values face_eq stores, in the form
 // store_cells takes them: deviations f - w for the fast form of shifted storage, else f.
-template <class P, bool FAST>
-__device__ __forceinline__ void eq_values(typename P::T br, typename P::T bux, typename P::T buy, typename P::T buz,
-                                          typename P::T (&out)[Q]) {
+template <class P, bool FAST, class A>
+__device__ __forceinline__ void eq_values(const A& a, typename P::T br, typename P::T bux, typename P::T buy,
+                                          typename P::T buz, typename P::T (&out)[Q]) {
     using T = typename P::T;
     const T bsq = (T)1.5 * (bux * bux + buy * buy + buz * buz);
     unroll<0, Q>([&](auto ic) {
@@ -651,7 +693,7 @@ __device__ __forceinline__ void eq_values(typename P::T br, typename P::T bux, t
         if constexpr (cz(i) < 0) s = s - buz;
         const T bc = (T)3.0 * s;
         const T v = (T)wd(i) * br * ((T)1.0 + bc + (T)0.5 * bc * bc - bsq);
-        if constexpr (P::shifted && FAST) out[i] = v - (T)wd(i);
+        if constexpr (P::shifted && FAST) out[i] = v - a.e[i];
         else out[i] = v;
     });
 }
@@ -667,7 +709,7 @@ __device__ __forceinline__ void collide_two(const StepArgs<typename P::S, typena
 #pragma unroll
         for (int i = 0; i < Q; ++i) g[i] = F2(f[0][i], f[1][i]);
         F2 ux, uy, uz, rho;
-        collide_fast<F2, P::shifted>(g, x0, a.nx, F2(a.tau), F2(a.csmag), ux, uy, uz, rho);
+        collide_fast<F2, P::shifted>(g, x0, a.nx, F2(a.tau), F2(a.csmag), shiftk2(a), ux, uy, uz, rho);
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             f[0][i] = g[i].v.x;
@@ -677,26 +719,26 @@ __device__ __forceinline__ void collide_two(const StepArgs<typename P::S, typena
         m[1][0] = ux.v.y; m[1][1] = uy.v.y; m[1][2] = uz.v.y; m[1][3] = rho.v.y;
     } else {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) collide_any<P, FAST>(f[k], x0 + k, a.nx, a.tau, a.csmag, m[k][0], m[k][1], m[k][2], m[k][3]);
+        for (int k = 0; k < 2; ++k) collide_any<P, FAST>(f[k], x0 + k, a.nx, a.tau, a.csmag, shiftk(a), m[k][0], m[k][1], m[k][2], m[k][3]);
     }
 }
 
 // Population I of V consecutive cells to p (aligned to V elements); half-width storage
 // rounds two values per conversion (each to nearest, as one at a time).
-template <class P, bool FAST, int V, int I>
-__device__ __forceinline__ void store_cells(typename P::S* p, const typename P::T (&f)[V][Q]) {
+template <class P, bool FAST, int V, int I, class A>
+__device__ __forceinline__ void store_cells(const A& a, typename P::S* p, const typename P::T (&f)[V][Q]) {
     using S = typename P::S;
     using T = typename P::T;
     if constexpr (V == 1) {
-        st_out<P, FAST, I>(p, f[0][I]);
+        st_out<P, FAST, I>(a, p, f[0][I]);
     } else {
         SVec<S, V> v;
 #pragma unroll
         for (int k = 0; k < V; k += 2) {
             T lo = f[k][I], hi = f[k + 1][I];
             if constexpr (P::shifted && !FAST) {
-                lo = lo - (T)wd(I);
-                hi = hi - (T)wd(I);
+                lo = lo - a.e[I];
+                hi = hi - a.e[I];
             }
             if constexpr (std::is_same<S, __half>::value) {
                 const __half2 h = __floats2half2_rn(lo, hi);
@@ -740,19 +782,19 @@ __device__ __forceinline__ void pair_load(const StepArgs<typename Prec<PREC>::S,
     r.codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
 }
 
-template <class P, bool FAST>
-__device__ __forceinline__ void pair_unpack(const PairRaw<typename P::S>& r, typename P::T (&f)[2][Q]) {
+template <class P, bool FAST, class A>
+__device__ __forceinline__ void pair_unpack(const A& a, const PairRaw<typename P::S>& r, typename P::T (&f)[2][Q]) {
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         if constexpr (cx(i) == 0) {
-            f[0][i] = ld_in<P, FAST, i>(&r.v[i].v[0]);
-            f[1][i] = ld_in<P, FAST, i>(&r.v[i].v[1]);
+            f[0][i] = ld_in<P, FAST, i>(a, &r.v[i].v[0]);
+            f[1][i] = ld_in<P, FAST, i>(a, &r.v[i].v[1]);
         } else if constexpr (cx(i) > 0) {
-            f[0][i] = ld_in<P, FAST, i>(&r.e[i]);
-            f[1][i] = ld_in<P, FAST, i>(&r.v[i].v[0]);
+            f[0][i] = ld_in<P, FAST, i>(a, &r.e[i]);
+            f[1][i] = ld_in<P, FAST, i>(a, &r.v[i].v[0]);
         } else {
-            f[0][i] = ld_in<P, FAST, i>(&r.v[i].v[1]);
-            f[1][i] = ld_in<P, FAST, i>(&r.e[i]);
+            f[0][i] = ld_in<P, FAST, i>(a, &r.v[i].v[1]);
+            f[1][i] = ld_in<P, FAST, i>(a, &r.e[i]);
         }
     });
 }
@@ -790,8 +832,9 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
                 if (((k ? c1 : c0) & CODE_NEAR) == 0) continue;
                 const int t = a.solid[idx0 + k - off];
                 if (t != 0) {
-                    // bounce-back; in deviation form w_opp(i) = w_i, so the value carries over
-                    T b = ld_in<P, FAST, opp(i)>(a.fin + (int64_t)opp(i) * a.n + idx0 + k);
+                    // bounce-back; in deviation form the shift difference e_opp(i) - e_i is added
+                    T b = ld_in<P, FAST, opp(i)>(a, a.fin + (int64_t)opp(i) * a.n + idx0 + k);
+                    if constexpr (FAST && P::shifted) b = b + a.bb[i];
                     if constexpr (cx(i) != 0) {
                         if (t == 2) b = b + (T)(6.0 * wd(i) * cx(i)) * a.uin;
                     }
@@ -806,26 +849,26 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
         m[0][0] = (T)0.0; m[0][1] = (T)0.0; m[0][2] = (T)0.0; m[0][3] = (T)1.0;
     }
     if (inlet && !sol0) {
-        eq_values<P, FAST>((T)1.0, a.uin, (T)0.0, (T)0.0, f[0]);
+        eq_values<P, FAST>(a, (T)1.0, a.uin, (T)0.0, (T)0.0, f[0]);
         m[0][0] = a.uin; m[0][1] = (T)0.0; m[0][2] = (T)0.0; m[0][3] = (T)1.0;
     }
     if (outlet && !sol1) {
         T br, bux, buy, buz;
         face_values<T>(nx - 1, y, z, nx, a.ny, a.nz, a.uin, m[0][0], m[0][1], m[0][2], m[0][3], br, bux, buy, buz);
-        eq_values<P, FAST>(br, bux, buy, buz, f[1]);
+        eq_values<P, FAST>(a, br, bux, buy, buz, f[1]);
         m[1][0] = bux; m[1][1] = buy; m[1][2] = buz; m[1][3] = br;
     }
     typename P::S* ob = a.dst[0] + idx0;  // population i of the output is at ob + i n
     if (!sol0 && !sol1) {
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            store_cells<P, FAST, 2, i>(ob + (int64_t)i * a.n, f);
+            store_cells<P, FAST, 2, i>(a, ob + (int64_t)i * a.n, f);
         });
     } else {
         const int32_t k = sol0 ? 1 : 0;  // the one fluid cell of the pair (selects, no indexing)
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            st_out<P, FAST, i>(ob + (int64_t)i * a.n + k, sol0 ? f[1][i] : f[0][i]);
+            st_out<P, FAST, i>(a, ob + (int64_t)i * a.n + k, sol0 ? f[1][i] : f[0][i]);
         });
     }
 #pragma unroll
@@ -854,7 +897,7 @@ __device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>
     if (!(sol0 && sol1)) {  // an all-solid pair pulls nothing
         PairRaw<typename P::S> r;
         pair_load<PREC>(a, idx0, r);
-        pair_unpack<P, FAST>(r, f);
+        pair_unpack<P, FAST>(a, r, f);
     }
     pair_finish<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, f);
 }
@@ -892,27 +935,27 @@ __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S
             constexpr int i = decltype(ic)::value;
             const S* p = a.src[i] + idx0;
             if constexpr (V == 1) {
-                f[0][i] = ld_in<P, FAST, i>(p);
+                f[0][i] = ld_in<P, FAST, i>(a, p);
             } else {
                 const SVec<S, V> v = vload<S, V>(p + cx(i));  // aligned: the shift cancels
                 if constexpr (cx(i) == 0) {
 #pragma unroll
-                    for (int k = 0; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k]);
+                    for (int k = 0; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(a, &v.v[k]);
                 } else if constexpr (cx(i) > 0) {
-                    f[0][i] = ld_in<P, FAST, i>(p);
+                    f[0][i] = ld_in<P, FAST, i>(a, p);
 #pragma unroll
-                    for (int k = 1; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k - 1]);
+                    for (int k = 1; k < V; ++k) f[k][i] = ld_in<P, FAST, i>(a, &v.v[k - 1]);
                 } else {
 #pragma unroll
-                    for (int k = 0; k < V - 1; ++k) f[k][i] = ld_in<P, FAST, i>(&v.v[k + 1]);
-                    f[V - 1][i] = ld_in<P, FAST, i>(p + V - 1);
+                    for (int k = 0; k < V - 1; ++k) f[k][i] = ld_in<P, FAST, i>(a, &v.v[k + 1]);
+                    f[V - 1][i] = ld_in<P, FAST, i>(a, p + V - 1);
                 }
             }
         });
         collide_cells<P, FAST, V>(a, f, idx0, x0, row_shell, mx, my, mz, mr);
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            store_cells<P, FAST, V, i>(a.dst[i] + idx0, f);
+            store_cells<P, FAST, V, i>(a, a.dst[i] + idx0, f);
         });
     } else if (valid) {
         // ---- general path: cell by cell (faces, inlet, outlet, solids, cells next to solids) ----
@@ -1108,10 +1151,10 @@ __device__ __forceinline__ SVec<S, 2> lds_pair(const S* p) {  // p aligned to 2 
     return r;
 }
 // the same from a shared-memory stage
-template <class P, bool FAST, int I>
-__device__ __forceinline__ typename P::T ld_in_smem(const typename P::S* p) {
+template <class P, bool FAST, int I, class A>
+__device__ __forceinline__ typename P::T ld_in_smem(const A& a, const typename P::S* p) {
     const typename P::S v = lds(p);
-    return ld_in<P, FAST, I>(&v);
+    return ld_in<P, FAST, I>(a, &v);
 }
 
 template <class S, int L>
@@ -1234,11 +1277,11 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
                     const S* sp = reinterpret_cast<const S*>(stage + i * LY::POP_BYTES) + a.chunk_r[i] + c;
                     if constexpr (cx(i) == 0) {  // chunk_r[i] == 0: an aligned pair
                         const SVec<S, 2> v = lds_pair(sp);
-                        f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
-                        f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
+                        f[0][i] = ld_in<P, FAST, i>(a, &v.v[0]);
+                        f[1][i] = ld_in<P, FAST, i>(a, &v.v[1]);
                     } else {
-                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
-                        f[1][i] = ld_in_smem<P, FAST, i>(sp + 1);
+                        f[0][i] = ld_in_smem<P, FAST, i>(a, sp);
+                        f[1][i] = ld_in_smem<P, FAST, i>(a, sp + 1);
                     }
                 });
                 if constexpr (CPT == 2) pair_finish<PREC, FAST>(a, idx, x, y, z, code, row_shell, f);
@@ -1248,20 +1291,20 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
                     constexpr int i = decltype(ic)::value;
                     const S* sp = reinterpret_cast<const S*>(stage + i * LY::POP_BYTES) + a.chunk_r[i] + c;
                     if constexpr (CPT == 1) {
-                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
+                        f[0][i] = ld_in_smem<P, FAST, i>(a, sp);
                     } else if constexpr (cx(i) == 0) {  // chunk_r[i] == 0: an aligned pair
                         const SVec<S, 2> v = lds_pair(sp);
-                        f[0][i] = ld_in<P, FAST, i>(&v.v[0]);
-                        f[1][i] = ld_in<P, FAST, i>(&v.v[1]);
+                        f[0][i] = ld_in<P, FAST, i>(a, &v.v[0]);
+                        f[1][i] = ld_in<P, FAST, i>(a, &v.v[1]);
                     } else {
-                        f[0][i] = ld_in_smem<P, FAST, i>(sp);
-                        f[1][i] = ld_in_smem<P, FAST, i>(sp + 1);
+                        f[0][i] = ld_in_smem<P, FAST, i>(a, sp);
+                        f[1][i] = ld_in_smem<P, FAST, i>(a, sp + 1);
                     }
                 });
                 collide_cells<P, FAST, CPT>(a, f, idx, x, row_shell, mx, my, mz, mr);
                 unroll<0, Q>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
-                    store_cells<P, FAST, CPT, i>(a.dst[i] + idx, f);
+                    store_cells<P, FAST, CPT, i>(a, a.dst[i] + idx, f);
                 });
             } else {
 #pragma unroll 1

@@ -84,7 +84,8 @@ class Solver:
     unseeded generator).
     """
 
-    def __init__(self, dims, device=None, precision='fp32', stream=None, seed=None, collision=None):
+    def __init__(self, dims, device=None, precision='fp32', stream=None, seed=None, collision=None,
+                 shift='free-stream'):
         self.dev = _device(device)
         self.nx, self.ny, self.nz = (int(d) for d in dims)
         self.n = n = self.nx * self.ny * self.nz
@@ -99,6 +100,9 @@ class Solver:
         if collision not in ('exact', 'fast'):
             raise ValueError(f'unknown collision form {collision!r}')
         self.collision = collision
+        if shift not in ('free-stream', 'rest'):
+            raise ValueError(f'unknown storage shift {shift!r}')
+        self.shift_mode = shift
         self.stream = stream if stream is not None else torch.cuda.Stream(self.dev)
         mac_dt = torch.float64 if self.precision == W.F64 else torch.float32
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
@@ -143,9 +147,16 @@ class Solver:
 
     # ---- set-up (server/lbm.py:415-440) ----
     def reset(self, uin):
-        """Equilibrium at rho = 1, u = (uin, 0, 0) in both population buffers (init_kernel)."""
+        """Equilibrium at rho = 1, u = (uin, 0, 0) in both population buffers (init_kernel).
+        fp16/bf16 storage is shifted by the equilibrium at u = (uin, 0, 0) from here on
+        (``shift_u``; 0 keeps the rest weights, e.g. for comparisons with that form)."""
+        if self.precision in (W.F16, W.BF16) and self.shift_mode == 'free-stream':
+            self.grid.shift_u = float(uin)
+        else:
+            self.grid.shift_u = 0.0
         for b in range(2):
-            call('wt_init_eq', self.precision, ptr(self.f[b]), ptr(self.mac[b]), self.n, float(uin), self.sh)
+            call('wt_init_eq', self.precision, ptr(self.f[b]), ptr(self.mac[b]), self.n, float(uin),
+                 float(self.grid.shift_u), self.sh)
 
     def set_solid(self, arr):
         """Upload the voxel mask (0 fluid, 1 solid, 2 moving belt) and rebuild the per-cell
@@ -383,7 +394,7 @@ class Solver:
         self.stream.synchronize()
         f = self.f[self.cur if which is None else which].double().cpu().numpy().reshape(Q, self.n)
         if self.precision in (W.F16, W.BF16):
-            f = f + np.array(_weights())[:, None]
+            f = f + shift_values(float(self.grid.shift_u)).astype(np.float64)[:, None]
         return f
 
     def macro(self):
@@ -414,6 +425,20 @@ class Solver:
             self.status_dev.zero_()
             torch.cuda.synchronize(self.dev)
         return v
+
+
+def shift_values(U):
+    """float32 e_i of shifted storage: w_i (1 + 3 c_xi U + 4.5 c_xi^2 U^2 - 1.5 U^2) evaluated
+    in double and rounded once (the library's ShiftTables); U = 0 gives w_i."""
+    w = _weights()
+    cxs = [0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0]
+    if U == 0.0:
+        return np.array(w, np.float32)
+    out = []
+    for i in range(Q):
+        cu = 3.0 * cxs[i] * U
+        out.append(w[i] * (1.0 + cu + 0.5 * cu * cu - 1.5 * U * U))
+    return np.array(out, np.float32)
 
 
 def _weights():

@@ -39,10 +39,11 @@ class Grid(ctypes.Structure):
                 ('f', ctypes.c_void_p * 2), ('mac', ctypes.c_void_p * 2),
                 ('solid', ctypes.c_void_p), ('code', ctypes.c_void_p),
                 ('tile', ctypes.c_int32), ('collision', ctypes.c_int32),
-                ('status', ctypes.c_void_p), ('test_skip_chunk', ctypes.c_int32), ('pad_', ctypes.c_int32)]
+                ('status', ctypes.c_void_p), ('test_skip_chunk', ctypes.c_int32), ('shift_u', ctypes.c_float)]
 
 
 _lib = None
+ABI_VERSION = 2  # include/wt.h WT_ABI_VERSION this binding is written against
 
 
 def lib():
@@ -59,7 +60,7 @@ def lib():
             'wt_abi_version': ([], ctypes.c_int),
             'wt_check_dims': ([i32, i32, i32], ctypes.c_int),
             'wt_population_bytes': ([i32, i64], i64),
-            'wt_init_eq': ([i32, vp, vp, i64, f64, vp], ctypes.c_int),
+            'wt_init_eq': ([i32, vp, vp, i64, f64, f64, vp], ctypes.c_int),
             'wt_build_codes': ([gp, vp], ctypes.c_int),
             'wt_links_scratch_len': ([i64], i64),
             'wt_links_scan': ([gp, vp, vp, vp], ctypes.c_int),
@@ -87,6 +88,8 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = res
+        if L.wt_abi_version() != ABI_VERSION:
+            raise RuntimeError(f'libwt.so ABI {L.wt_abi_version()} != {ABI_VERSION}; rebuild wind-tunnel_b200')
         _lib = L
     return _lib
 
