@@ -55,7 +55,7 @@ class FakeBatch:
         assert not self.closed
         self.clock.t += sum(s.s.n for s in self.solvers) * k / self.rate
 
-    def event(self):
+    def event(self, timing=False):
         return None
 
     def close(self):

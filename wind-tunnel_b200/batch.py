@@ -71,10 +71,11 @@ class TunnelBatch:
         self._wait_members()
         call('wt_batch_replay', self.handle, self.sh)
 
-    def event(self):
+    def event(self, timing=False):
         """A CUDA event recorded after the work queued so far on the batch stream; member
-        Solvers wait on it (Solver.wait_event) before their frame kernels."""
-        e = torch.cuda.Event()
+        Solvers wait on it (Solver.wait_event) before their frame kernels. With timing, two
+        such events give the device time between them (Event.elapsed_time)."""
+        e = torch.cuda.Event(enable_timing=timing)
         e.record(self.stream)
         return e
 

@@ -85,8 +85,10 @@ class SessionServer:
         self.collision = collision
         self.period = 1.0 / fps
         self.steps_per_frame = int(steps_per_frame)
-        # batched tile: two cells per thread at 64 registers unless chosen (fp64 spills there)
-        self.tile = int(tile) if tile else (2 if precision == 'fp64' else 18)
+        # batched tile: two cells per thread, 256 threads, 80 registers (the fastest batched
+        # shape in fp32 and fp16; the batch descriptor's fields take registers that a single
+        # tunnel's constant-bank parameters do not), one cell per thread for fp64
+        self.tile = int(tile) if tile else (2 if precision == 'fp64' else 7)
         self.clock = clock
         self.solver_factory = solver_factory or self._make_solver
         self.batch_factory = batch_factory or self._make_batch
@@ -111,6 +113,8 @@ class SessionServer:
         self._stream = None
         self.phase = {'admit': 0.0, 'rebuild': 0.0, 'issue': 0.0, 'collect': 0.0}
         self.round_s = []
+        self.step_gpu_s = 0.0  # device time of the batched steps (CUDA events on the batch stream)
+        self.step_cells = 0
 
     # ---- default factories (the GPU path) ----
     def _make_solver(self, s):
@@ -192,8 +196,9 @@ class SessionServer:
             self.rebuilds += 1
         t_rebuild = self.clock()
         k = self.steps_per_frame
+        started = self._batch.event(timing=True)
         self._batch.step(k)
-        done = self._batch.event()
+        done = self._batch.event(timing=True)
         for s in due:
             s.solver.wait_event(done)
             s.solver.advance_particles(k, s.p)
@@ -221,6 +226,9 @@ class SessionServer:
             # the client acknowledges at once and asks again at its next 1/fps tick
             s.request_t = max(t, s.request_t + self.period)
         t_end = self.clock()
+        if started is not None:  # every frame has been collected, so both events are complete
+            self.step_gpu_s += started.elapsed_time(done) / 1e3
+            self.step_cells += sum(s.n for s in due) * k
         for name, a, b in (('admit', now, t_admit), ('rebuild', t_admit, t_rebuild), ('issue', t_rebuild, t_issue),
                            ('collect', t_issue, t_end)):
             self.phase[name] += b - a
@@ -243,6 +251,8 @@ class SessionServer:
                 'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
                 'peak_used_gb': round(self.peak_used / 1e9, 2),
                 'glups': round(self.cell_updates / span / 1e9, 3),
+                'step_glups_device': round(self.step_cells / max(1e-9, self.step_gpu_s) / 1e9, 3),
+                'step_share_of_wall': round(self.step_gpu_s / span, 3),
                 'round_ms': {'p50': round(float(np.percentile(rs, 50)), 1), 'p99': round(float(np.percentile(rs, 99)), 1),
                              **{f'{k}_mean': round(v / max(1, self.rounds) * 1e3, 2) for k, v in self.phase.items()}},
                 'frames_per_session_s': round(len(self.latencies) / span / max(1e-9, self.active_sum / max(1, self.rounds)), 2)}
@@ -252,6 +262,8 @@ class SessionServer:
         self.latencies.clear()
         self.round_s.clear()
         self.phase = dict.fromkeys(self.phase, 0.0)
+        self.step_gpu_s = 0.0
+        self.step_cells = 0
         self.cell_updates = 0
         self.rounds = self.active_sum = 0
         self.t0 = self.clock()
