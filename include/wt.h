@@ -168,6 +168,19 @@ int wt_batch_replay(wt_batch* b, void* stream);
 int wt_batch_cur(const wt_batch* b, int32_t* cur_out);
 int wt_batch_destroy(wt_batch* b);
 
+/* ---- server-side voxeliser (web/js/voxelize.js:5-115) ---- */
+/* voxelize(): a triangle soup in lattice coordinates (tris: num_tris x 9 floats, device) to a
+ * mask (solid: n bytes, device): ray parity along +x, surface shell, flood fill of fluid from
+ * the boundary, then the y = 0 layer tagged 2 when ground != 0. Arithmetic in double in the
+ * reference's order; triangles with a non-finite coordinate are skipped. out4 (host) receives
+ * frontal area, planform area, solid cell count (before the ground layer) and the number of
+ * ray crossings. The workspace (device, 256-byte aligned) holds up to max_crossings crossings;
+ * with fewer, the call returns WT_ERR_CAPACITY with the needed number in out4[3]. The call
+ * synchronises `stream` (a set-up step). */
+int64_t wt_voxelize_workspace_bytes(int32_t nx, int32_t ny, int32_t nz, int64_t max_crossings);
+int wt_voxelize(const float* tris, int64_t num_tris, int32_t nx, int32_t ny, int32_t nz, int32_t ground,
+                uint8_t* solid, void* workspace, int64_t workspace_bytes, int64_t* out4, void* stream);
+
 /* ---- frame outputs (Solver.frame, server/lbm.py:458-482) ---- */
 /* advect_kernel (server/lbm.py:233-263): RK2 streamline particles through mac.
  * Respawn uses this library's counter-based RNG (not Warp's). mac: float (4*n). */

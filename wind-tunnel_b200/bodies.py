@@ -167,3 +167,38 @@ def config4(count=24, seed=4, cells=(0.5e6, 8e6)):
         nu = float(rng.uniform(0.001, 0.01))
         out.append((dims, solid, dict(uIn=u0, tau=3.0 * nu + 0.5, smag=0.16)))
     return out
+
+
+# ---- triangle meshes (lattice coordinates) for the voxeliser ----
+def box_mesh(lo, hi):
+    """Closed axis-aligned box [lo, hi] as 12 triangles, float32 (12, 9)."""
+    (x0, y0, z0), (x1, y1, z1) = lo, hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], np.float64)
+    quads = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (3, 7, 6, 2), (0, 4, 7, 3), (1, 2, 6, 5)]
+    tris = []
+    for a, b, c, d in quads:
+        tris += [v[[a, b, c]].reshape(-1), v[[a, c, d]].reshape(-1)]
+    return np.array(tris, np.float32)
+
+
+def ellipsoid_mesh(centre, semi, n_lat=24, n_lon=48):
+    """Closed UV-tessellated ellipsoid, float32 (T, 9): rings of latitude between the poles."""
+    cx, cy, cz = centre
+    a, b, c = semi
+    th = np.linspace(0.0, np.pi, n_lat + 1)
+    ph = np.linspace(0.0, 2.0 * np.pi, n_lon + 1)
+
+    def pt(i, j):
+        return (cx + a * np.sin(th[i]) * np.cos(ph[j]), cy + b * np.cos(th[i]), cz + c * np.sin(th[i]) * np.sin(ph[j]))
+
+    tris = []
+    for i in range(n_lat):
+        for j in range(n_lon):
+            p00, p01, p10, p11 = pt(i, j), pt(i, j + 1), pt(i + 1, j), pt(i + 1, j + 1)
+            if i > 0:
+                tris.append(p00 + p10 + p01)
+            if i < n_lat - 1:
+                tris.append(p01 + p10 + p11)
+    return np.array(tris, np.float32)
+

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 OUT = os.path.join(HERE, 'libwt.so')
-SOURCES = ['wt_abi.cu', 'wt_setup.cu', 'wt_step.cu', 'wt_batch.cu', 'wt_reduce.cu', 'wt_frame.cu']
+SOURCES = ['wt_abi.cu', 'wt_setup.cu', 'wt_step.cu', 'wt_batch.cu', 'wt_reduce.cu', 'wt_frame.cu', 'wt_voxel.cu']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-O3', '-std=c++17', '-fmad=false',
          '-Xcompiler', '-fPIC', '-Xcompiler', '-O2', '--ptxas-options=-v', '-ccbin', 'g++']

@@ -23,7 +23,8 @@ EXPORTS = ['wt_last_error', 'wt_abi_version', 'wt_check_dims', 'wt_population_by
            'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step_tiles', 'wt_step',
            'wt_reduce_scratch_len', 'wt_forces', 'wt_forces_noalloc', 'wt_mass', 'wt_batch_workspace_bytes',
            'wt_batch_create', 'wt_batch_step', 'wt_batch_capture', 'wt_batch_replay', 'wt_batch_cur',
-           'wt_batch_destroy', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp']
+           'wt_batch_destroy', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp',
+           'wt_voxelize_workspace_bytes', 'wt_voxelize']
 
 
 class WtError(RuntimeError):
@@ -83,6 +84,8 @@ def lib():
             'wt_pack_particles': ([vp, vp, vp, vp, i32, i32, i32, i64, vp], ctypes.c_int),
             'wt_slice': ([vp, vp, vp, i32, i32, i32, i32, i32, i32, f32, f32, f32, f32, vp], ctypes.c_int),
             'wt_cp': ([vp, vp, vp, vp, vp, i32, i32, i32, i64, f32, f32, vp], ctypes.c_int),
+            'wt_voxelize_workspace_bytes': ([i32, i32, i32, i64], ctypes.c_int64),
+            'wt_voxelize': ([vp, i64, i32, i32, i32, i32, vp, vp, i64, vp, vp], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
