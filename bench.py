@@ -273,6 +273,7 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.empty_cache()
 
     batching = run_batching(dev) if args.batch and prec == 'fp32' else None
+    vox = run_voxelize(dev) if args.batch and prec == 'fp32' else None
 
     acc = None
     if args.accuracy and prec == 'fp32' and rank == 0:
@@ -281,7 +282,7 @@ def run_ours(args, rank, world, local_rank):
                'laminar_nu0.02': accuracy.study(steps=2 * args.accuracy_steps, scale=0.5, device=dev, nu=0.02)}
 
     return dict(value=value, t_dev=t_dev, roofline=roofline, e2e=e2e, clocks=clk.summary(), accuracy=acc,
-                batching=batching,
+                batching=batching, voxelize=vox,
                 launches=launches_per_frame * args.steps, dims=dims, n=n, variants=variants)
 
 
@@ -344,6 +345,30 @@ def run_batching(dev, replays=5, graph_steps=100):
     del solvers, alone
     torch.cuda.empty_cache()
     return out
+
+
+def run_voxelize(dev, repeats=3):
+    """Server-side voxeliser (web/js/voxelize.js on the GPU) on the benchmark body: the six
+    ellipsoids of the 512x256x256 workload as triangle meshes, timed end to end (mesh upload,
+    all stages, mask and areas back on the host), and compared with the analytic mask of the
+    same ellipsoids (they differ only in surface cells)."""
+    import bodies
+    import voxel
+    dims = (512, 256, 256)
+    analytic, params = bodies.ellipsoid_union(dims, 6, 2024, scale=1.0, floor='belt')
+    tris = np.concatenate([bodies.ellipsoid_mesh((cx, cy, cz), (a, b, c), 48, 96) for cx, cy, cz, a, b, c in params])
+    voxel.voxelize(tris, dims, ground=True, device=dev)  # warm-up (module load, allocator)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        solid, st = voxel.voxelize(tris, dims, ground=True, device=dev)
+        times.append(time.perf_counter() - t0)
+    n = dims[0] * dims[1] * dims[2]
+    differ = int((solid != analytic).sum())
+    return {'dims': list(dims), 'triangles': int(len(tris)), 'crossings': st['crossings'],
+            'ms': round(min(times) * 1e3, 2), 'gcells_per_s': round(n / min(times) / 1e9, 3),
+            'solid_cells': st['count'], 'frontal': st['frontal'], 'planform': st['planform'],
+            'cells_differing_from_analytic': differ, 'fraction_differing': round(differ / n, 6)}
 
 
 def cpu_baseline(dims, solid, budget_s, threads=None):
@@ -438,7 +463,7 @@ def main():
                    'parallelism': f'replicas x{world}'},
         'roofline': r['roofline'], 'cpu_baseline': cpu, 'e2e': r['e2e'], 'clocks': r['clocks'],
         'gpu_launches': r['launches'], 'precision_variants': r['variants'], 'accuracy_vs_fp64': r['accuracy'],
-        'batching': r['batching'], 'serving': serving_out,
+        'batching': r['batching'], 'voxelize': r['voxelize'], 'serving': serving_out,
     }
     print(json.dumps(line), flush=True)
 
