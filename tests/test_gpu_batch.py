@@ -63,3 +63,23 @@ def test_batch_graph_replay_equals_steps():
         assert np.array_equal(s.populations(), f)
         assert np.array_equal(s.macro(), mac)
     b.close()
+
+
+@pytest.mark.parametrize('collision,precision', [('exact', 'fp32'), ('fast', 'fp16')])
+def test_streams_executor_equals_tunnels_alone(collision, precision):
+    """mode='streams': every tunnel stepped by its own kernel on its own stream, at once."""
+    from batch import TunnelBatch
+    tun = _tunnels(collision, precision)
+    b = TunnelBatch([t[0] for t in tun], [t[2] for t in tun], mode='streams')
+    b.step(3)
+    b.step(4)
+    b.event().synchronize()
+    for s, solid, p in tun:
+        f, mac = _alone((s.nx, s.ny, s.nz), solid, p, 7, collision, precision)
+        assert s.cur == 1
+        assert np.array_equal(s.populations(), f)
+        assert np.array_equal(s.macro(), mac)
+    with pytest.raises(NotImplementedError):
+        b.capture(2)
+    b.close()
+

@@ -44,12 +44,13 @@ def _alone(s, frames, precision, k):
     return out
 
 
+@pytest.mark.parametrize('mode', ['streams', 'persistent'])
 @pytest.mark.parametrize('precision', ['fp32', 'fp16'])
-def test_each_session_same_alone_and_in_the_mix(precision):
+def test_each_session_same_alone_and_in_the_mix(precision, mode):
     import serving
     clock = Clock()
     srv = serving.SessionServer('cuda:0', budget_bytes=1e9, precision=precision, clock=clock, keep_frames=True,
-                                tile=2)
+                                tile=2, batch_mode=mode)
     ss = _sessions()
     srv.submit(ss[0])
     srv.submit(ss[1])

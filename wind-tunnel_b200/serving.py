@@ -13,9 +13,10 @@ owns a tunnel on one GPU:
   one when it has its previous frame and its 1/fps tick has come: the reference's `ready`
   flow control (server/app.py:173-193) with 30 fps pacing.
 * **Rounds.** A round takes every session with an outstanding request. Their tunnels advance
-  ``steps_per_frame`` steps together in one ``TunnelBatch`` (one persistent bulk kernel per
-  step over a tile work-list that spans every tunnel, then one face kernel); the batch is
-  rebuilt only when the set of sessions changes. Then each session's stream waits for the
+  ``steps_per_frame`` steps together in one ``TunnelBatch``: by default each tunnel's own
+  kernel on its own stream, all running at once (``batch_mode='streams'``), or one persistent
+  bulk kernel per step over a tile work-list spanning every tunnel (``'persistent'``); the
+  batch is rebuilt only when the set of sessions changes. Then each session's stream waits for the
   batch, advects its particles and runs its frame kernels, which write the wire-format frame
   straight into one device buffer (``Solver.launch_frame_packed``), and one copy brings it
   back. Frames are collected in session order. Sessions admitted while a round runs join
@@ -78,7 +79,7 @@ class SessionServer:
 
     def __init__(self, device='cuda:0', budget_bytes=160e9, precision='fp32', fps=30.0, steps_per_frame=10,
                  tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
-                 footprint=None, keep_frames=False):
+                 footprint=None, keep_frames=False, batch_mode='streams'):
         self.device = device
         self.budget = float(budget_bytes)
         self.precision = precision
@@ -89,6 +90,9 @@ class SessionServer:
         # shape in fp32 and fp16; the batch descriptor's fields take registers that a single
         # tunnel's constant-bank parameters do not), one cell per thread for fp64
         self.tile = int(tile) if tile else (2 if precision == 'fp64' else 7)
+        # executor of the round's steps: every tunnel's own kernel on its own stream, all at
+        # once ('streams', the faster on uneven mixes) or one persistent batched kernel
+        self.batch_mode = batch_mode
         self.clock = clock
         self.solver_factory = solver_factory or self._make_solver
         self.batch_factory = batch_factory or self._make_batch
@@ -132,7 +136,7 @@ class SessionServer:
         from batch import TunnelBatch
         if self._stream is None:
             self._stream = torch.cuda.Stream(torch.device(self.device))
-        return TunnelBatch(solvers, params, tile=self.tile, stream=self._stream)
+        return TunnelBatch(solvers, params, tile=self.tile, stream=self._stream, mode=self.batch_mode)
 
     # ---- admission ----
     def submit(self, session):
