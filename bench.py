@@ -290,7 +290,9 @@ def run_batching(dev, replays=5, graph_steps=100):
     """Config 4: 24 tunnels (0.5M-8M cells, 2:1:1, own obstacles and flow parameters) in one
     batch: persistent bulk kernel over a tile work-list plus a face kernel per step, captured
     as a CUDA graph of `graph_steps` steps. The batch tile is picked by timing each batched
-    tile shape. One tunnel is then re-run alone and compared bit for bit."""
+    tile shape. The streams executor (every tunnel's own kernel on its own stream, forked and
+    joined inside one graph) is timed the same way. One tunnel is then re-run alone, for
+    every step both executors made, and compared bit for bit."""
     import torch
     import bodies
     import lbm
@@ -330,6 +332,21 @@ def run_batching(dev, replays=5, graph_steps=100):
     steps_done += replays * graph_steps
     t = ev0.elapsed_time(ev1) / 1e3
     b.close()
+    # the streams executor: each tunnel's own kernel on its own stream, all at once, the
+    # fork and join captured as one graph of the same length
+    b = TunnelBatch(solvers, params, mode='streams')
+    b.capture(graph_steps)
+    b.replay()
+    steps_done += graph_steps
+    b.synchronize()
+    ev0.record(b.stream)
+    for _ in range(replays):
+        b.replay()
+    ev1.record(b.stream)
+    ev1.synchronize()
+    steps_done += replays * graph_steps
+    ts = ev0.elapsed_time(ev1) / 1e3
+    b.close()
     k = min(range(len(solvers)), key=lambda i: solvers[i].n)
     dims, solid, p = cfg[k]
     alone = lbm.Solver(dims, dev)
@@ -341,6 +358,8 @@ def run_batching(dev, replays=5, graph_steps=100):
            'tile_ms_per_step': {str(a): round(v, 3) for a, v in tile_ms.items()},
            'graph_steps': graph_steps, 'replays': replays, 'ms_per_step': round(t / (replays * graph_steps) * 1e3, 4),
            'glups': round(cells * replays * graph_steps / t / 1e9, 3),
+           'streams': {'ms_per_step': round(ts / (replays * graph_steps) * 1e3, 4),
+                       'glups': round(cells * replays * graph_steps / ts / 1e9, 3)},
            'checked_tunnel': list(dims), 'checked_steps': steps_done, 'bit_identical_to_alone': same}
     del solvers, alone
     torch.cuda.empty_cache()

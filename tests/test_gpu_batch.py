@@ -79,7 +79,21 @@ def test_streams_executor_equals_tunnels_alone(collision, precision):
         assert s.cur == 1
         assert np.array_equal(s.populations(), f)
         assert np.array_equal(s.macro(), mac)
-    with pytest.raises(NotImplementedError):
-        b.capture(2)
+    b.close()
+
+
+def test_streams_executor_graph_replay_equals_steps():
+    from batch import TunnelBatch
+    tun = _tunnels('fast', 'fp16')
+    b = TunnelBatch([t[0] for t in tun], [t[2] for t in tun], mode='streams')
+    b.capture(10)
+    b.replay()
+    b.replay()
+    b.event().synchronize()
+    for s, solid, p in tun:
+        f, mac = _alone((s.nx, s.ny, s.nz), solid, p, 20, 'fast', 'fp16')
+        assert s.cur == 0
+        assert np.array_equal(s.populations(), f)
+        assert np.array_equal(s.macro(), mac)
     b.close()
 

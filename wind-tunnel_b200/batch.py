@@ -7,7 +7,8 @@ executors:
   spans every tunnel, then one kernel over all tunnels' face cells; ``capture(k)`` records k
   (even) steps as a CUDA graph that ``replay()`` launches with a single call.
 * ``mode='streams'``: each tunnel is stepped by the single-tunnel kernel on its own stream, all
-  streams running at once after the batch stream's prior work, and the batch stream joins them.
+  streams running at once after the batch stream's prior work, and the batch stream joins them;
+  ``capture(k)`` records that fork and join (k even) as one CUDA graph.
   Each kernel keeps its tunnel's scalars in its constant-bank parameters, so it runs the
   64-register two-cell tile; concurrent tunnels fill each other's tails. On a mix of 0.5-33.5M
   tunnels this executor is the faster one (fp16 60.6 vs 40.5 GLUPS).
@@ -94,13 +95,40 @@ class TunnelBatch:
         call('wt_batch_step', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
         self._sync_cur()
 
+    def _capture_streams(self, steps, mac_all_last):
+        # the batch stream forks to every member stream and joins back inside one graph; an
+        # even step count returns every tunnel to the buffer it started from, so replays chain
+        if steps <= 0 or steps % 2:
+            raise ValueError('capture needs an even, positive step count')
+        self._wait_members()
+        self.stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        flags = W.STEP_MAC_ALL_LAST if mac_all_last else 0
+        with torch.cuda.graph(g, stream=self.stream):
+            start = torch.cuda.Event()
+            start.record(self.stream)
+            for s, p in zip(self.solvers, self.params):
+                s.stream.wait_event(start)
+                call('wt_step', s.gp, s.cur, int(steps), float(p['uIn']), float(p['tau']), float(p['smag']), flags,
+                     s.sh)
+            for s in self.solvers:
+                self.stream.wait_stream(s.stream)
+        self._graph = g
+
     def capture(self, steps, mac_all_last=True):
         if self.mode == 'streams':
-            raise NotImplementedError('graph capture is the persistent executor\'s (mode="persistent")')
+            self._capture_streams(steps, mac_all_last)
+            return
         call('wt_batch_capture', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
 
     def replay(self):
         self._wait_members()
+        if self.mode == 'streams':
+            if getattr(self, '_graph', None) is None:
+                raise RuntimeError('replay before capture')
+            with torch.cuda.stream(self.stream):
+                self._graph.replay()
+            return
         call('wt_batch_replay', self.handle, self.sh)
 
     def event(self, timing=False):
@@ -117,6 +145,7 @@ class TunnelBatch:
     def close(self):
         if self.mode == 'streams':
             self.stream.synchronize()
+            self._graph = None
             return
         if self.handle:
             self.stream.synchronize()
