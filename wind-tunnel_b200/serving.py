@@ -327,23 +327,38 @@ class Arrivals:
 
 
 def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='fp32', seed=5, device='cuda:0',
-             particles=5000, warm_start=True, tile=0, steps_per_frame=10, fps=30.0, mask_set=None):
+             particles=5000, warm_start=True, tile=0, steps_per_frame=10, fps=30.0, mask_set=None, keep=None,
+             before_window=None, latencies_out=None, server_factory=None):
     """Config 5 in wall-clock time: Poisson arrivals at `rate` per second for `duration`
     seconds, each session requesting `fps` frames per second of its particles, one slice and
     Cd/Cl, admitted against `budget` bytes. With warm_start the run begins from the arrival
     process's stationary population (Poisson with mean rate x mean_life sessions; lifetimes
     are memoryless, so their residual lifetimes are exponential with the same mean), so the
-    window measures the steady state; the set-up of those sessions is not timed."""
+    window measures the steady state; the set-up of those sessions is not timed.
+
+    For one GPU of several (placement.py): ``keep(session, t)`` is asked about every session
+    of the arrival stream, t its arrival in seconds from the start of the window (0 for the
+    stationary ones), and only the sessions it accepts are served here; ``before_window()``
+    runs between the set-up and the window (a barrier across GPUs); ``latencies_out`` (a list)
+    receives the window's frame latencies in seconds. ``server_factory`` replaces the
+    SessionServer constructor (same arguments)."""
     gen = Arrivals(seed, mean_life, particles, mask_set)
-    srv = SessionServer(device, budget_bytes=budget, precision=precision, fps=fps,
-                        steps_per_frame=steps_per_frame, tile=tile)
+    srv = (server_factory or SessionServer)(device, budget_bytes=budget, precision=precision, fps=fps,
+                                            steps_per_frame=steps_per_frame, tile=tile)
+
+    def offer(s, t):
+        if keep is None or keep(s, t):
+            srv.submit(s)
+
     start = time.perf_counter()
     if warm_start:
         for _ in range(int(gen.rng.poisson(rate * mean_life))):
-            srv.submit(gen.session(start))
+            offer(gen.session(start), 0.0)
         srv._admit(start)
         srv.round()  # the stationary sessions have been running: one round builds their batch
     setup_s = time.perf_counter() - start
+    if before_window is not None:
+        before_window()
     t0 = time.perf_counter()
     for s in srv.active.values():  # the window starts now; set-up time is not service time
         s.arrival += t0 - start
@@ -360,13 +375,16 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     while time.perf_counter() < t0 + duration:
         now = time.perf_counter()
         while arrivals and arrivals[0] <= now:
-            srv.submit(gen.session(heapq.heappop(arrivals)))
+            t = heapq.heappop(arrivals)
+            offer(gen.session(t), t - t0)
         if srv.round() == 0:
             time.sleep(0.0005)
     out = srv.stats()
     out.update(precision=precision, duration_s=duration, arrival_rate=rate, mean_lifetime_s=mean_life,
                budget_gb=budget / 1e9, warm_start=warm_start, steps_per_frame=steps_per_frame, fps=fps,
                particles=particles, setup_s=round(setup_s, 1))
+    if latencies_out is not None:
+        latencies_out.extend(srv.latencies)
     srv.close()
     return out
 
