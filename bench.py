@@ -140,7 +140,6 @@ def build_workload(scale):
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    import torch.distributed as dist
     import lbm
 
     dev = torch.device('cuda', local_rank)
@@ -151,16 +150,11 @@ def run_ours(args, rank, world, local_rank):
     p = frame_params(dims)
     prec = args.precision
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    import ranks
+    barrier = ranks.barrier
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max_over_ranks(x, dev)
 
     # ---- device-resident frame loop ----
     s = lbm.Solver(dims, dev, precision=prec, seed=1234 + rank, collision=args.collision)
@@ -194,7 +188,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
     barrier()
     t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    value = world * n * STEPS_PER_FRAME * args.steps / t_dev / 1e9
+    value = ranks.whole_job_rate(n * STEPS_PER_FRAME * args.steps, t_dev) / 1e9
 
     # ---- LBM step alone: roofline of the fused step (bulk + face kernels) ----
     nstep = max(20, args.steps)
@@ -241,7 +235,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     t_e2e = max_over_ranks(time.perf_counter() - t0)
     h2d_total = solid.nbytes + verts.nbytes + norms.nbytes + N_PARTICLES * 16
-    e2e = {'value': round(world * n * STEPS_PER_FRAME * args.steps / t_e2e / 1e9, 3), 'unit': 'GLUPS',
+    e2e = {'value': round(ranks.whole_job_rate(n * STEPS_PER_FRAME * args.steps, t_e2e) / 1e9, 3), 'unit': 'GLUPS',
            'h2d_bytes_per_step': int(round(h2d_total / args.steps)), 'd2h_bytes_per_step': int(d2h),
            'what': 'one session through lbm.Solver: set_solid + set_surface + reset + set_particles, then K frames of '
                    'step(10) + frame() with outputs copied to pinned host memory',
