@@ -55,6 +55,27 @@ def peaks():
         return 6650.0, 'fallback'
 
 
+def copy_bandwidth(dev, nbytes=2 << 30, reps=5):
+    """Device-to-device copy bandwidth on this GPU now (read + write bytes per second, GB/s):
+    torch's copy of a buffer 16x larger than L2, best of `reps`, CUDA events."""
+    import torch
+    src = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    dst = torch.empty_like(src)
+    src.fill_(1)
+    dst.copy_(src)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float('inf')
+    for _ in range(reps):
+        ev0.record()
+        dst.copy_(src)
+        ev1.record()
+        ev1.synchronize()
+        best = min(best, ev0.elapsed_time(ev1) / 1e3)
+    del src, dst
+    torch.cuda.empty_cache()
+    return 2 * nbytes / best / 1e9
+
+
 def profile_traffic(name):
     """dram bytes per launch from a committed ncu summary (profiles/<name>), if present."""
     path = os.path.join(ROOT, 'profiles', name)
@@ -200,12 +221,14 @@ def run_ours(args, rank, world, local_rank):
     t_step = ev0.elapsed_time(ev1) / 1e3 / nstep
     hbm, peak_kind = peaks()
     achieved = ALGO_BYTES[prec] * n / t_step / 1e9
+    copy_here = copy_bandwidth(dev)
     traffic = profile_traffic(f'step_{prec}_{nx}x{ny}x{nz}.md')
     roofline = {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': hbm, 'unit': 'GB/s',
                 'frac': round(achieved / hbm, 4), 'traffic': traffic,
                 'peak_source': f'{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)' if peak_kind == 'measured'
                 else 'fallback 6.65 TB/s', 'kernel': f'wt_step ({prec}) = k_step_bulk + k_step_faces, one LBM step',
                 'algorithmic_bytes_per_cell': ALGO_BYTES[prec], 'step_ms': round(t_step * 1e3, 4),
+                'copy_gbs_this_run': round(copy_here, 1), 'frac_of_copy_this_run': round(achieved / copy_here, 4),
                 'glups_step_only': round(n / t_step / 1e9, 3), 'tile': tile,
                 'tile_ms_per_step': {str(k): round(v, 4) for k, v in tile_ms.items()}}
     del s
