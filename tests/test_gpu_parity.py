@@ -175,6 +175,64 @@ def test_random_obstacles_match_oracle(oracle_mod, prec_name, oprec, shift, dims
     np.testing.assert_allclose(s.mass(), L.mass(), rtol=1e-13)
 
 
+def _degenerate(name):
+    """Grids at and near the smallest the library accepts, and masks with nothing to do."""
+    if name == 'min_4x3x3_fluid':
+        return (4, 3, 3), np.zeros(36, np.uint8)
+    if name == 'min_4x3x3_belt':
+        s = np.zeros(36, np.uint8)
+        s.reshape(3, 3, 4)[:, 0, :] = 2
+        return (4, 3, 3), s
+    if name == 'row_34x3x3':  # one interior row
+        return (34, 3, 3), _random_case((34, 3, 3), 21)
+    if name == 'short_4x10x7':  # the inlet and outlet columns are neighbours of one interior pair
+        return (4, 10, 7), _random_case((4, 10, 7), 22)
+    if name == 'thin_6x3x5':
+        return (6, 3, 5), _random_case((6, 3, 5), 23)
+    if name == 'all_solid_10x5x5':
+        return (10, 5, 5), np.ones(250, np.uint8)
+    if name == 'one_fluid_cell_8x5x5':
+        s = np.ones(200, np.uint8)
+        s[3 + 8 * (2 + 5 * 2)] = 0
+        return (8, 5, 5), s
+    raise KeyError(name)
+
+
+DEGENERATE = ['min_4x3x3_fluid', 'min_4x3x3_belt', 'row_34x3x3', 'short_4x10x7', 'thin_6x3x5', 'all_solid_10x5x5',
+              'one_fluid_cell_8x5x5']
+
+
+@pytest.mark.parametrize('prec_name,oprec', [('fp32', 0), ('fp16', 1), ('fp64', 3)])
+@pytest.mark.parametrize('case', DEGENERATE)
+def test_degenerate_grids_match_oracle(oracle_mod, case, prec_name, oprec):
+    """Smallest and thinnest grids (every cell a face or next to one), an all-solid mask and a
+    single fluid cell, in every admissible tile, bit for bit against the oracle."""
+    import autotune
+    dims, solid = _degenerate(case)
+    uin, tau, smag = 0.07, 0.52, 0.16
+    p = dict(uIn=uin, tau=tau, smag=smag)
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name)
+    L = oracle_mod.Lattice(dims, oprec, shift_u=float(np.float32(uin)) if oprec in (1, 2) else 0.0)
+    L.solid[:] = solid
+    L.reset(uin)
+    L.step(6, uin, tau, smag)
+    tiles = [t[0] for t in autotune.admissible(s)]
+    assert tiles
+    for tile in tiles:
+        s.set_tile(tile)
+        s.reset(uin)
+        s.cur = 0
+        for chunk in (1, 2, 3):
+            s.step(chunk, p)
+        s.synchronize()
+        assert np.array_equal(s.f[s.cur].cpu().numpy(), L.f[L.cur]), f'{case} tile {tile}'
+        assert np.array_equal(s.mac[s.cur].cpu().numpy(), L.mac), f'{case} tile {tile}'
+    _, d64, b64 = L.forces()
+    f6 = s.forces6()
+    np.testing.assert_allclose(f6[:3], d64, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(s.mass(), L.mass(), rtol=1e-13)
+
+
 def test_link_list_matches_mask():
     dims = (48, 20, 18)
     solid = _random_case(dims, 9)
