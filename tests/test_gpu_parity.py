@@ -127,6 +127,70 @@ def test_frame_kernels_match_reference():
     assert len(out['forces']) == 3
 
 
+def test_frame_kernels_at_the_edges():
+    """Slices of the first and last plane of every axis (and indices outside, which the Solver
+    clamps as server/lbm.py:467 does), particles packed and advected at and beyond the domain
+    edges, and surface points at the corners and outside, against the oracle."""
+    import oracle
+    dims = (20, 9, 7)
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    rng = np.random.default_rng(31)
+    solid = _random_case(dims, 31)
+    mac = np.empty((n, 4), np.float32)
+    mac[:, :3] = rng.uniform(-0.12, 0.12, (n, 3))
+    mac[:, 3] = rng.uniform(0.9, 1.1, n)
+    s = _solver(dict(dims=np.array(dims), solid=solid), 'fp32')
+    s.mac[s.cur].copy_(torch.from_numpy(mac))
+    torch.cuda.synchronize()
+    uin = 0.06
+    p = dict(uIn=uin, tau=0.51, smag=0.16, lref=6.0, maxAge=50.0, seedX=2.0, seedCy=4.0, seedCz=3.0, seedHy=2.5,
+             seedHz=2.0)
+    for axis in range(3):
+        dim = dims[axis]
+        for index in (0, dim - 1, -4, dim + 5):
+            for field in range(4):
+                p['slice'] = dict(axis=axis, index=index, field=field, vmin=0.0, vmax=1.4)
+                out = s.frame(p, want_cp=False)
+                ref = oracle.slice_(mac, solid, dims, axis, max(0, min(dim - 1, index)), field, uin, p['lref'], 0.0,
+                                    1.4)
+                assert np.array_equal(out['slice'], ref), (axis, index, field)
+    p['slice'] = None
+    # particles on the faces, corners and outside; speeds at and beyond the packing range
+    xs = [0.0, nx - 1.0, -3.0, nx + 2.5, 0.5, nx - 3.0, 1e6, -1e6]
+    ys = [0.0, ny - 1.0, ny + 4.0, -2.0, 0.5, ny - 1.5]
+    zs = [0.0, nz - 1.0, -1.0, nz + 3.0, 0.5, nz - 1.5]
+    pos = np.array([(x, y, z, a) for x in xs for y in ys for z in zs for a in (0.0, 3.0)], np.float32)
+    spd = np.resize(np.array([0.0, 1.99, 2.0, 5.0, -1.0, 0.004], np.float32), len(pos))
+    s.num_p = len(pos)
+    s.pos = torch.from_numpy(pos.copy()).cuda()
+    s.spd = torch.from_numpy(spd.copy()).cuda()
+    s.q16 = torch.zeros(s.num_p * 4, dtype=torch.int16, device='cuda')
+    s.q8 = torch.zeros(s.num_p, dtype=torch.uint8, device='cuda')
+    torch.cuda.synchronize()
+    out = s.frame(p, want_cp=False)
+    q16, q8 = oracle.pack(pos, spd, dims)
+    assert np.array_equal(out['parts16'].view(np.uint16), q16)
+    assert np.array_equal(out['parts8'], q8)
+    s.seed = 40
+    s._advect(3.0, p)
+    s.synchronize()
+    pos_o, spd_o = pos.copy(), spd.copy()
+    oracle.advect(pos_o, spd_o, mac, solid, dims, 3.0, uin, p['maxAge'], 40, p['seedX'], p['seedCy'], p['seedCz'],
+                  p['seedHy'], p['seedHz'])
+    assert np.array_equal(s.pos.cpu().numpy(), pos_o)
+    assert np.array_equal(s.spd.cpu().numpy(), spd_o)
+    # surface points at the corners, on the faces and outside, normals along each axis and diagonals
+    verts = np.array([(x, y, z) for x in (0.0, nx - 1.0, -2.0, nx + 1.0, 3.3) for y in (0.0, ny - 1.0, 4.6)
+                      for z in (0.0, nz - 1.0, -1.5, 2.2)], np.float32)
+    dirs = np.array([(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1), (0.6, 0.8, 0),
+                     (0, -0.6, 0.8)], np.float32)
+    norms = np.resize(dirs, (len(verts), 3)).astype(np.float32)
+    s.set_surface(verts, norms)
+    out = s.frame(p, want_cp=True)
+    assert np.array_equal(out['cp'], oracle.cp(mac, solid, verts, norms, dims, uin))
+
+
 def _random_case(dims, seed, belt=True):
     rng = np.random.default_rng(seed)
     nx, ny, nz = dims
