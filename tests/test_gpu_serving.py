@@ -50,7 +50,7 @@ def test_each_session_same_alone_and_in_the_mix(precision, mode):
     import serving
     clock = Clock()
     srv = serving.SessionServer('cuda:0', budget_bytes=1e9, precision=precision, clock=clock, keep_frames=True,
-                                tile=2, batch_mode=mode)
+                                tile=2, batch_mode=mode, rate_in_header=False)
     ss = _sessions()
     srv.submit(ss[0])
     srv.submit(ss[1])
@@ -73,3 +73,105 @@ def test_each_session_same_alone_and_in_the_mix(precision, mode):
             assert a == b, f'session {s.id} frame {j} differs from the session run alone'
     assert np.isfinite([s.cd for s in ss]).all()
     srv.close()
+
+
+def _engine_replay(s0, script, precision, mode, rounds):
+    """One session alone, driven as the reference Engine drives its Solver (server/app.py:
+    104-193): commands, then step(steps) when running, then a frame (Cp every third frame)."""
+    import gzip
+    import numpy as np
+    import wire
+    from lbm import Solver
+    p = dict(s0.p)
+    sv = Solver(s0.dims, 'cuda:0', precision=precision, seed=s0.id)
+    sv.set_solid(s0.solid)
+    sv.reset(p['uIn'])
+    sv.set_particles(s0.particles, p)
+    particles = s0.particles
+    frames, frame_no = [], 0
+    for r in range(rounds):
+        for msg, payload in script.get((r, s0.id), []):
+            t = msg['type']
+            if t == 'params':
+                old = int(p.get('particles', particles))
+                p.update({k: v for k, v in msg.items() if k != 'type'})
+                new = int(p.get('particles', old))
+                if new != old:
+                    particles = new
+                    if sv.num_p:
+                        sv.set_particles(new, p)
+            elif t == 'reset':
+                sv.reset(p['uIn'])
+            elif t == 'respawn':
+                sv.set_particles(int(p.get('particles', particles)), p)
+            else:
+                got = wire.upload_arrays(msg, payload, s0.dims)
+                if got[0] == 'solid':
+                    sv.set_solid(got[1])
+                else:
+                    sv.set_surface(got[1], got[2])
+        running = bool(p.get('running', True))
+        k = (int(p.get('steps', 10)) if mode == 'streams' else 10) if running else 0
+        if k:
+            sv.step(k, p)
+        frame_no += 1
+        every = max(3, sv.num_verts // 20000)
+        want_cp = bool(p.get('cp')) and sv.num_verts > 0 and frame_no % every == 0
+        sv.launch_frame_packed(p, want_cp)
+        header = dict(type='frame', dims=list(s0.dims), numP=sv.num_p, numVerts=sv.num_verts, forces=None, steps=k,
+                      mlups=0.0, running=running)
+        frames.append(sv.collect_frame_packed(header))
+    return frames
+
+
+@pytest.mark.parametrize('mode', ['streams', 'persistent'])
+def test_client_commands_match_the_engine_semantics(mode):
+    """Two sessions under client pacing receive parameter changes, a reset, a respawn, a mask
+    and a surface upload, a pause and a resume, through SessionServer.command; every frame
+    equals the frame the same session gets alone when the same commands are applied the way
+    the reference's Engine applies them."""
+    import copy
+    import numpy as np
+    import bodies
+    import serving
+    import wire
+    ss = _sessions()[:2]
+    for s in ss:
+        s.lifetime = 1e9
+    originals = [copy.deepcopy(s) for s in ss]
+    new_solid, _ = bodies.ellipsoid_union(ss[1].dims, 3, 977, scale=ss[1].dims[0] / 256.0, floor='belt')
+    verts, norms = bodies.surface_points(ss[0].solid, ss[0].dims)
+    surf = np.concatenate([verts.reshape(-1), norms.reshape(-1)]).astype(np.float32).tobytes()
+    up = lambda h, b: wire.decode_upload(wire.encode_upload(h, b))
+    script = {
+        (1, 0): [({'type': 'params', 'uIn': 0.065, 'steps': 6, 'cp': True}, None),
+                 up({'type': 'surface', 'numVerts': len(verts)}, surf)],
+        (1, 1): [up({'type': 'solid', 'dims': list(ss[1].dims)}, new_solid.tobytes())],
+        (2, 0): [({'type': 'reset'}, None), ({'type': 'respawn'}, None)],
+        (2, 1): [({'type': 'params', 'running': False}, None)],
+        (4, 1): [({'type': 'params', 'running': True, 'particles': 120}, None)],
+        (5, 0): [({'type': 'params', 'tau': 0.56}, None)],
+    }
+    rounds = 7
+    clock = Clock()
+    srv = serving.SessionServer('cuda:0', budget_bytes=1e9, precision='fp32', clock=clock, keep_frames=True,
+                                batch_mode=mode, pacing='client', rate_in_header=False)
+    for s in ss:
+        srv.submit(s)
+    for r in range(rounds):
+        clock.t = r * 0.1
+        for sid in (0, 1):
+            if r:
+                srv.command(sid, {'type': 'ready'})
+            for msg, payload in script.get((r, sid), []):
+                srv.command(sid, msg, payload)
+        assert srv.round() == 2
+    got = {0: [], 1: []}
+    for sid, frame in srv.frame_log:
+        got[sid].append(frame)
+    srv.close()
+    for s0 in originals:
+        want = _engine_replay(s0, script, 'fp32', mode, rounds)
+        assert len(got[s0.id]) == rounds
+        for r, (a, b) in enumerate(zip(got[s0.id], want)):
+            assert a == b, f'session {s0.id} frame {r}'

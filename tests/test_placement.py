@@ -71,6 +71,7 @@ class _FakeSolver:
     def __init__(self, s):
         self.num_p = s.particles
         self.last_forces6 = [0.0] * 6
+        self.num_verts = 0
 
     def device_bytes(self):
         return 0

@@ -19,8 +19,25 @@ class FakeSolver:
         self.s = s
         self.num_p = s.particles
         self.last_forces6 = [0.0] * 6
+        self.num_verts = 0 if s.verts is None else len(s.verts)
         self.launched = 0
         self.advanced = 0
+        self.calls = []
+        self.cp_frames = []
+
+    def set_particles(self, count, p):
+        self.num_p = count
+        self.calls.append(('set_particles', count))
+
+    def reset(self, uin):
+        self.calls.append(('reset', uin))
+
+    def set_solid(self, solid):
+        self.calls.append(('set_solid', bytes(solid)))
+
+    def set_surface(self, verts, norms):
+        self.num_verts = len(verts)
+        self.calls.append(('set_surface', len(verts)))
 
     def device_bytes(self):
         return 0
@@ -33,6 +50,8 @@ class FakeSolver:
 
     def launch_frame_packed(self, p, want_cp):
         self.launched += 1
+        if want_cp:
+            self.cp_frames.append(self.launched)
 
     def collect_frame_packed(self, header):
         return repr((self.s.id, self.launched, sorted(header))).encode()
@@ -51,9 +70,13 @@ class FakeBatch:
         self.closed = False
         FakeBatch.log.append(tuple(s.s.id for s in solvers))
 
+    steps = []
+
     def step(self, k):
         assert not self.closed
-        self.clock.t += sum(s.s.n for s in self.solvers) * k / self.rate
+        FakeBatch.steps.append(k)
+        ks = k if isinstance(k, list) else [k] * len(self.solvers)
+        self.clock.t += sum(s.s.n * kk for s, kk in zip(self.solvers, ks)) / self.rate
 
     def event(self, timing=False):
         return None
@@ -62,11 +85,12 @@ class FakeBatch:
         self.closed = True
 
 
-def _server(clock, rate=1e12, budget=100.0):
+def _server(clock, rate=1e12, budget=100.0, **kw):
     FakeBatch.log = []
+    FakeBatch.steps = []
     return serving.SessionServer(device=None, budget_bytes=budget, clock=clock, solver_factory=FakeSolver,
                                  batch_factory=lambda sv, p: FakeBatch(clock, rate, sv),
-                                 footprint=lambda s: float(s.n))
+                                 footprint=lambda s: float(s.n), **kw)
 
 
 def _session(sid, n, life=1e9, arrival=0.0):
@@ -145,3 +169,125 @@ def test_arrival_joins_next_round_and_batch_rebuilds():
     srv.round()
     assert FakeBatch.log == [(0,), (0, 1)]
     assert srv.active[1].frames == 1 and srv.active[0].frames == 2
+
+
+# ---- client commands (server/app.py:104-149, routed to the client's session) ----
+def _upload(header, payload):
+    import wire
+    return wire.decode_upload(wire.encode_upload(header, payload))
+
+
+def test_commands_run_at_the_next_round_in_order():
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 4))
+    srv.round()
+    sv = srv.active[0].solver
+    srv.command(0, {'type': 'params', 'uIn': 0.08, 'particles': 9})
+    srv.command(0, {'type': 'reset'})
+    srv.command(0, {'type': 'respawn'})
+    assert sv.calls == []  # nothing before the round
+    c.t += 1 / 30
+    srv.round()
+    assert sv.calls == [('set_particles', 9), ('reset', 0.08), ('set_particles', 9)]
+    assert srv.active[0].p['uIn'] == 0.08
+    assert FakeBatch.log == [(0,), (0,)]  # new flow parameters: the batch is rebuilt
+
+
+def test_uploads_checked_like_the_engine():
+    import numpy as np
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 4))  # dims (4, 1, 1)
+    srv.round()
+    sv = srv.active[0].solver
+    good = np.array([0, 1, 2, 0], np.uint8)
+    srv.command(0, *_upload({'type': 'solid', 'dims': [4, 1, 1]}, good.tobytes()))
+    srv.command(0, *_upload({'type': 'solid', 'dims': [5, 1, 1]}, np.zeros(5, np.uint8).tobytes()))  # other grid
+    srv.command(0, *_upload({'type': 'solid', 'dims': [4, 1, 1]}, np.zeros(3, np.uint8).tobytes()))  # short
+    verts = np.arange(12, dtype=np.float32).reshape(2, 6)
+    srv.command(0, *_upload({'type': 'surface', 'numVerts': 2}, verts.tobytes()))
+    srv.command(0, *_upload({'type': 'surface', 'numVerts': 3}, verts.tobytes()))  # size mismatch
+    c.t += 1 / 30
+    srv.round()
+    assert sv.calls == [('set_solid', good.tobytes()), ('set_surface', 2)]
+    assert np.array_equal(srv.active[0].solid, good)
+    with pytest.raises(ValueError):
+        srv.command(0, {'type': 'grid', 'res': 'high'})
+
+
+def test_queued_session_keeps_its_commands():
+    import numpy as np
+    c = Clock()
+    srv = _server(c, budget=4)
+    srv.submit(_session(0, 4, life=1.0))
+    srv.submit(_session(1, 4))
+    srv.round()
+    srv.command(1, {'type': 'params', 'tau': 0.6})
+    srv.command(1, *_upload({'type': 'solid', 'dims': [4, 1, 1]}, np.ones(4, np.uint8).tobytes()))
+    srv.command(7, {'type': 'reset'})  # no such session: ignored
+    c.t = 1.0
+    srv.round()
+    s1 = srv.active[1]
+    assert s1.p['tau'] == 0.6 and np.array_equal(s1.solid, np.ones(4, np.uint8))
+    assert s1.solver.calls == []  # created from the updated session, nothing replayed
+
+
+def test_client_pacing_waits_for_ready():
+    c = Clock()
+    srv = _server(c, pacing='client')
+    srv.submit(_session(0, 2))
+    for _ in range(3):
+        srv.round()
+        c.t += 0.01
+    assert srv.active[0].frames == 1
+    srv.command(0, {'type': 'ready'})
+    srv.round()
+    assert srv.active[0].frames == 2
+    assert srv.latencies[-1] < 1e-6  # requested at the ack, served in the same round
+
+
+def test_paused_session_is_not_stepped_and_frames_slow_down():
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 2))
+    srv.submit(_session(1, 2))
+    srv.command(1, {'type': 'params', 'running': False})
+    while c.t < 1.0:
+        srv.round()
+        c.t += 0.001
+    a, b = srv.active[0], srv.active[1]
+    assert a.solver.advanced == 10 * a.frames and b.solver.advanced == 0
+    assert 29 <= a.frames <= 31 and 11 <= b.frames <= 13  # paused sessions at 12 Hz
+    assert all(key == (0,) for key in FakeBatch.log)
+
+
+def test_per_session_steps_with_the_streams_executor():
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 2))
+    srv.submit(_session(1, 2))
+    srv.command(1, {'type': 'params', 'steps': 4})
+    srv.round()
+    assert FakeBatch.steps == [[10, 4]]
+    assert srv.active[1].solver.advanced == 4
+    p = _server(c, batch_mode='persistent')
+    p.submit(_session(0, 2))
+    p.submit(_session(1, 2))
+    p.command(1, {'type': 'params', 'steps': 4})
+    p.round()
+    assert FakeBatch.steps == [10]  # one launch steps every tunnel alike
+
+
+def test_surface_pressure_every_third_frame():
+    import numpy as np
+    c = Clock()
+    srv = _server(c)
+    s = _session(0, 2)
+    s.p['cp'] = True
+    srv.submit(s)
+    srv.command(0, *_upload({'type': 'surface', 'numVerts': 1}, np.zeros(6, np.float32).tobytes()))
+    for _ in range(7):
+        srv.round()
+        c.t += 1 / 30
+    assert srv.active[0].solver.cp_frames == [3, 6]

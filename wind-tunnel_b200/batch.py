@@ -81,16 +81,29 @@ class TunnelBatch:
         start = torch.cuda.Event()
         start.record(self.stream)
         flags = W.STEP_MAC_ALL_LAST if mac_all_last else 0
-        for s, p in zip(self.solvers, self.params):
+        for s, p, k in zip(self.solvers, self.params, steps):
+            if k <= 0:
+                continue
             s.stream.wait_event(start)
-            call('wt_step', s.gp, s.cur, int(steps), float(p['uIn']), float(p['tau']), float(p['smag']), flags, s.sh)
-            s.cur ^= int(steps) & 1
+            call('wt_step', s.gp, s.cur, int(k), float(p['uIn']), float(p['tau']), float(p['smag']), flags, s.sh)
+            s.cur ^= int(k) & 1
         self._wait_members()
 
     def step(self, steps, mac_all_last=True):
+        """Advance every tunnel `steps` steps; with the streams executor `steps` may also be one
+        count per tunnel (each tunnel is its own launch)."""
+        if isinstance(steps, (list, tuple)):
+            if len(steps) != len(self.solvers):
+                raise ValueError('one step count per tunnel')
+            counts = [int(k) for k in steps]
+            if self.mode != 'streams' and len(set(counts)) > 1:
+                raise ValueError('the persistent executor steps every tunnel alike')
+        else:
+            counts = [int(steps)] * len(self.solvers)
         if self.mode == 'streams':
-            self._step_streams(steps, mac_all_last)
+            self._step_streams(counts, mac_all_last)
             return
+        steps = counts[0]
         self._wait_members()
         call('wt_batch_step', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
         self._sync_cur()

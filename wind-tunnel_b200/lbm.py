@@ -178,8 +178,9 @@ class Solver:
         self.stream.synchronize()
 
     def set_surface(self, verts, norms):
-        verts = np.ascontiguousarray(np.asarray(verts, np.float32).reshape(-1, 3))
-        norms = np.ascontiguousarray(np.asarray(norms, np.float32).reshape(-1, 3))
+        # writable copies where needed: uploads arrive as read-only views of the message bytes
+        verts = np.require(np.asarray(verts, np.float32).reshape(-1, 3), requirements=['C', 'W'])
+        norms = np.require(np.asarray(norms, np.float32).reshape(-1, 3), requirements=['C', 'W'])
         self.num_verts = len(verts)
         with torch.cuda.stream(self.stream):
             self.verts = torch.from_numpy(verts).to(self.dev, non_blocking=False)
@@ -304,12 +305,22 @@ class Solver:
         return self.collect_frame()
 
     def _frame_buffers(self, layout, wh):
-        key = (self.num_p, wh, layout.total_bytes)
-        if getattr(self, '_pk_layout_key', None) != key:
+        # grow-only: frames with and without surface pressure alternate layouts, and pinned
+        # allocation is slow. A new layout zeroes the device buffer, so the padding between
+        # parts is zero, as pack() writes it.
+        key = (self.num_p, wh, layout.total_bytes, tuple(sorted(layout.offsets.items())))
+        if getattr(self, '_pk_layout_key', None) == key:
+            return
+        need = layout.total_bytes
+        if getattr(self, '_pk_cap', 0) < need:
             with torch.cuda.stream(self.stream):
-                self._pk_dev = torch.zeros(layout.total_bytes, dtype=torch.uint8, device=self.dev)
-            self._pk_host = torch.empty(layout.total_bytes, dtype=torch.uint8, pin_memory=True)
-            self._pk_layout_key = key
+                self._pk_dev = torch.zeros(need, dtype=torch.uint8, device=self.dev)
+            self._pk_host = torch.empty(need, dtype=torch.uint8, pin_memory=True)
+            self._pk_cap = need
+        else:
+            with torch.cuda.stream(self.stream):
+                self._pk_dev.zero_()
+        self._pk_layout_key = key
 
     def _frame_layout(self, p, want_cp):
         sl = p.get('slice')
@@ -355,7 +366,8 @@ class Solver:
         call('wt_forces', self.gp, self.cur, ptr(self.link_cells), ptr(self.link_masks), self.n_links,
              ptr(self.partials), base + layout.forces_offset, self.sh)
         with torch.cuda.stream(self.stream):
-            self._pk_host.copy_(self._pk_dev, non_blocking=True)
+            tb = layout.total_bytes
+            self._pk_host[:tb].copy_(self._pk_dev[:tb], non_blocking=True)
             self._pk_event = torch.cuda.Event()
             self._pk_event.record(self.stream)
         self._pk_pending = (layout, extra)

@@ -21,6 +21,15 @@ owns a tunnel on one GPU:
   straight into one device buffer (``Solver.launch_frame_packed``), and one copy brings it
   back. Frames are collected in session order. Sessions admitted while a round runs join
   the next round, so their work overlaps everyone else's from then on.
+* **Commands.** ``command(session, msg, payload)`` takes a client's messages as the Engine's
+  handle() does (server/app.py:104-149): 'params' (flow parameters, particle count,
+  'running', 'steps', 'cp'), 'respawn', 'reset', 'ready' and the 'solid' / 'surface' uploads
+  (checked by wire.upload_arrays). They run in arrival order when the next round starts. A
+  paused session is not stepped and gets frames at 12 Hz; with the streams executor each
+  session steps its own 'steps' per frame; surface pressure comes every third frame when
+  'cp' is on (server/app.py:177-178). With ``pacing='client'`` a session's next frame waits for
+  its client's 'ready', as in the reference; the default ``'fps'`` stands in for clients that
+  acknowledge at once and ask again at their next 1/fps tick.
 * **Latency.** A frame's latency runs from its request to the moment its bytes are on the
   host. ``stats()`` gives p50/p99 over all frames, admitted/retired/abandoned/queued counts,
   the peak and end memory in use, and the aggregate lattice-update rate over the window.
@@ -38,6 +47,9 @@ import numpy as np
 
 import bodies
 import lbm
+import wire
+
+PAUSED_HZ = 12  # frames per second of a paused session (server/app.py:20)
 
 
 class Session:
@@ -67,6 +79,14 @@ class Session:
         self.steps = 0
         self.cd = self.cl = float('nan')
         self.last_frame = None
+        self.mlups = 0.0
+        self.frame_no = 0
+        self.ready = True          # client pacing: the client holds no unacknowledged frame
+        self.verts = self.norms = None  # surface points for Cp, once uploaded
+
+    @property
+    def running(self):
+        return bool(self.p.get('running', True))
 
 
 class SessionServer:
@@ -79,7 +99,8 @@ class SessionServer:
 
     def __init__(self, device='cuda:0', budget_bytes=160e9, precision='fp32', fps=30.0, steps_per_frame=10,
                  tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
-                 footprint=None, keep_frames=False, batch_mode='streams'):
+                 footprint=None, keep_frames=False, batch_mode='streams', pacing='fps', paused_hz=PAUSED_HZ,
+                 rate_in_header=True):
         self.device = device
         self.budget = float(budget_bytes)
         self.precision = precision
@@ -98,6 +119,14 @@ class SessionServer:
         self.batch_factory = batch_factory or self._make_batch
         self.footprint = footprint or (lambda s: lbm.estimate_bytes(s.dims, precision, s.particles))
         self.keep_frames = keep_frames
+        # 'fps': each client asks for its next frame at its next 1/fps tick (the simulated
+        # clients of config 5); 'client': only after it acknowledges the last one ('ready')
+        if pacing not in ('fps', 'client'):
+            raise ValueError(f'unknown pacing {pacing!r}')
+        self.pacing = pacing
+        self.paused_period = 1.0 / paused_hz
+        self.rate_in_header = rate_in_header
+        self._cmds = []           # (session id, message, payload) in arrival order
         self.active = {}          # id -> Session, in admission order
         self.queue = []           # FIFO of sessions waiting for memory
         self.used = 0.0
@@ -127,7 +156,9 @@ class SessionServer:
         sv.reset(s.p['uIn'])
         if s.particles:
             sv.set_particles(s.particles, s.p)
-        sv.prepare_frame(s.p, False)
+        if s.verts is not None:
+            sv.set_surface(s.verts, s.norms)
+        sv.prepare_frame(s.p, s.verts is not None)
         sv.synchronize()
         return sv
 
@@ -137,6 +168,91 @@ class SessionServer:
         if self._stream is None:
             self._stream = torch.cuda.Stream(torch.device(self.device))
         return TunnelBatch(solvers, params, tile=self.tile, stream=self._stream, mode=self.batch_mode)
+
+    # ---- client commands (server/app.py:104-149, one session each) ----
+    def command(self, sid, msg, payload=None):
+        """Queue a client's command for its session: the JSON messages 'params', 'respawn',
+        'reset' and 'ready', or an upload 'solid' / 'surface' with its gzip payload (the two
+        halves wire.decode_upload returns). Commands run in arrival order at the start of the
+        next round, as the reference's Engine drains its queue before it steps. A session still
+        waiting for memory keeps its parameters and uploads for when it is admitted. A
+        resolution change ('grid') is a new session: its footprint goes through admission."""
+        if msg.get('type') == 'grid':
+            raise ValueError("a resolution change is a new session; submit one")
+        self._cmds.append((sid, dict(msg), payload))
+
+    def _invalidate(self, s):
+        # a batched tunnel's parameters, buffers or mask changed: rebuild the batch
+        if self._batch is not None and self._batch_key is not None and s.id in self._batch_key:
+            self._batch.close()
+            self._batch, self._batch_key = None, None
+
+    def _apply_commands(self, now):
+        cmds, self._cmds = self._cmds, []
+        for sid, msg, payload in cmds:
+            s = self.active.get(sid)
+            if s is None:
+                s = next((q for q in self.queue if q.id == sid), None)
+            if s is None:
+                continue  # gone, or never here: the reference ignores commands without a solver
+            self._apply(s, msg, payload, now)
+
+    def _apply(self, s, msg, payload, now):
+        t = msg.get('type')
+        sv = s.solver
+        if t == 'ready':
+            if not s.ready:
+                s.ready = True
+                s.request_t = now
+        elif t == 'params':
+            old = int(s.p.get('particles', s.particles))
+            s.p.update({k: v for k, v in msg.items() if k != 'type'})
+            new = int(s.p.get('particles', old))
+            if new != old:
+                s.particles = new
+                if sv is not None and sv.num_p:
+                    sv.set_particles(new, s.p)
+            self._invalidate(s)
+        elif t == 'respawn':
+            if sv is not None:
+                sv.set_particles(int(s.p.get('particles', s.particles)), s.p)
+        elif t == 'reset':
+            if sv is not None:
+                self._invalidate(s)
+                sv.reset(s.p['uIn'])
+        elif t in ('solid', 'surface'):
+            got = wire.upload_arrays(msg, payload, s.dims)
+            if got is None:
+                return
+            if got[0] == 'solid':
+                s.solid = got[1].copy()
+                if sv is not None:
+                    self._invalidate(s)
+                    sv.set_solid(s.solid)
+            else:
+                s.verts, s.norms = got[1].copy(), got[2].copy()
+                if sv is not None:
+                    sv.set_surface(s.verts, s.norms)
+
+    def _frame_steps(self, s):
+        """Steps before a session's next frame: none while paused; its own 'steps' with the
+        streams executor (each tunnel its own launch); the server's steps_per_frame with the
+        persistent one (one launch steps every tunnel alike)."""
+        if not s.running:
+            return 0
+        if self.batch_mode == 'streams':
+            return int(s.p.get('steps', self.steps_per_frame))
+        return self.steps_per_frame
+
+    def _due(self, s, now):
+        if self.pacing == 'client':
+            return s.ready and (s.running or now - s.last_t >= self.paused_period)
+        return s.request_t <= now
+
+    def _want_cp(self, s):
+        # the Engine's surface pressure cadence (server/app.py:177-178)
+        every = max(3, s.solver.num_verts // 20000)
+        return bool(s.p.get('cp')) and s.solver.num_verts > 0 and s.frame_no % every == 0
 
     # ---- admission ----
     def submit(self, session):
@@ -184,34 +300,44 @@ class SessionServer:
         now = self.clock()
         if self.t0 is None:
             self.t0 = now
+        self._apply_commands(now)
         self._retire(now)
         self._admit(now)
         t_admit = self.clock()
-        due = [s for s in self.active.values() if s.request_t <= now]
+        due = [s for s in self.active.values() if self._due(s, now)]
         if not due:
             self.phase['admit'] += t_admit - now
             return 0
-        key = tuple(s.id for s in due)
-        if key != self._batch_key:
-            if self._batch is not None:
-                self._batch.close()
-            self._batch = self.batch_factory([s.solver for s in due], [s.p for s in due])
-            self._batch_key = key
-            self.rebuilds += 1
+        ks = {s.id: self._frame_steps(s) for s in due}
+        stepping = [s for s in due if ks[s.id] > 0]
+        started = done = None
+        if stepping:
+            key = tuple(s.id for s in stepping)
+            if key != self._batch_key:
+                if self._batch is not None:
+                    self._batch.close()
+                self._batch = self.batch_factory([s.solver for s in stepping], [s.p for s in stepping])
+                self._batch_key = key
+                self.rebuilds += 1
         t_rebuild = self.clock()
-        k = self.steps_per_frame
-        started = self._batch.event(timing=True)
-        self._batch.step(k)
-        done = self._batch.event(timing=True)
+        if stepping:
+            counts = [ks[s.id] for s in stepping]
+            started = self._batch.event(timing=True)
+            self._batch.step(counts[0] if len(set(counts)) == 1 else counts)
+            done = self._batch.event(timing=True)
         for s in due:
-            s.solver.wait_event(done)
-            s.solver.advance_particles(k, s.p)
-            s.solver.launch_frame_packed(s.p, False)
+            k = ks[s.id]
+            if k:
+                s.solver.wait_event(done)
+                s.solver.advance_particles(k, s.p)
+            s.frame_no += 1
+            s.solver.launch_frame_packed(s.p, self._want_cp(s))
         t_issue = self.clock()
         for s in due:
             sv = s.solver
-            header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=0, forces=None, steps=k,
-                          mlups=0.0, running=True)
+            k = ks[s.id]
+            header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=sv.num_verts, forces=None, steps=k,
+                          mlups=s.mlups if (self.rate_in_header and s.running) else 0.0, running=s.running)
             t_prev = s.last_t
             frame = sv.collect_frame_packed(header)
             t = self.clock()
@@ -227,12 +353,15 @@ class SessionServer:
             q = 0.5 * s.p['uIn'] ** 2 * max(1, s.frontal)  # the client's Cd/Cl (web/js/main.js:337-339)
             s.cd, s.cl = fx / q, fy / q
             s.mlups = s.n * k / max(1e-9, t - t_prev) / 1e6
-            # the client acknowledges at once and asks again at its next 1/fps tick
-            s.request_t = max(t, s.request_t + self.period)
+            if self.pacing == 'client':
+                s.ready = False  # until the client acknowledges this frame
+            else:
+                # the client acknowledges at once and asks again at its next tick
+                s.request_t = max(t, s.request_t + (self.period if s.running else self.paused_period))
         t_end = self.clock()
         if started is not None:  # every frame has been collected, so both events are complete
             self.step_gpu_s += started.elapsed_time(done) / 1e3
-            self.step_cells += sum(s.n for s in due) * k
+            self.step_cells += sum(s.n * ks[s.id] for s in stepping)
         for name, a, b in (('admit', now, t_admit), ('rebuild', t_admit, t_rebuild), ('issue', t_rebuild, t_issue),
                            ('collect', t_issue, t_end)):
             self.phase[name] += b - a

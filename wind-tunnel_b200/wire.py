@@ -89,3 +89,42 @@ class FrameLayout:
         """Frame bytes from a payload buffer laid out by this layout."""
         hb = header_bytes(header, self.offsets)
         return struct.pack('<I', len(hb)) + hb + bytes(memoryview(payload)[:self.payload_bytes])
+
+
+# ---- client to server: geometry uploads (web/js/net.js:9-16, 85-92; server/app.py:218-222) ----
+def encode_upload(header, payload):
+    """A client's binary message: [u32 LE header length][JSON header][gzip of payload], as
+    the browser's frameBytes(header, await gzip(bytes)) builds it."""
+    import gzip
+    hb = json.dumps(header).encode()
+    return struct.pack('<I', len(hb)) + hb + gzip.compress(bytes(payload))
+
+
+def decode_upload(buf):
+    """(header dict, compressed payload bytes) of a client's binary message, split as the
+    reference's WebSocket handler splits it (server/app.py:218-222)."""
+    buf = bytes(buf)
+    hl = struct.unpack_from('<I', buf, 0)[0]
+    return json.loads(buf[4:4 + hl]), buf[4 + hl:]
+
+
+def upload_arrays(header, payload, dims):
+    """The arrays an upload carries, checked as Engine.handle checks them (server/app.py:
+    138-148): ('solid', u8[n]) for a mask of exactly this grid, ('surface', verts, norms) for
+    numVerts vertices and normals, or None for anything the reference ignores (another grid's
+    mask, a size mismatch, an unknown type)."""
+    import gzip
+    t = header.get('type')
+    nx, ny, nz = dims
+    if t == 'solid':
+        if tuple(header.get('dims', ())) != (nx, ny, nz):
+            return None
+        arr = np.frombuffer(gzip.decompress(payload), dtype=np.uint8)
+        return ('solid', arr) if arr.size == nx * ny * nz else None
+    if t == 'surface':
+        raw = np.frombuffer(gzip.decompress(payload), dtype=np.float32)
+        nv = int(header['numVerts'])
+        if raw.size != nv * 6:
+            return None
+        return 'surface', raw[:nv * 3].reshape(-1, 3), raw[nv * 3:].reshape(-1, 3)
+    return None
