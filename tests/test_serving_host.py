@@ -241,9 +241,11 @@ def test_client_pacing_waits_for_ready():
         srv.round()
         c.t += 0.01
     assert srv.active[0].frames == 1
+    assert srv.round_frames == []
     srv.command(0, {'type': 'ready'})
     srv.round()
     assert srv.active[0].frames == 2
+    assert [sid for sid, _ in srv.round_frames] == [0]
     assert srv.latencies[-1] < 1e-6  # requested at the ack, served in the same round
 
 

@@ -127,6 +127,7 @@ class SessionServer:
         self.paused_period = 1.0 / paused_hz
         self.rate_in_header = rate_in_header
         self._cmds = []           # (session id, message, payload) in arrival order
+        self.round_frames = []    # (session id, frame bytes) produced by the latest round
         self.active = {}          # id -> Session, in admission order
         self.queue = []           # FIFO of sessions waiting for memory
         self.used = 0.0
@@ -300,6 +301,7 @@ class SessionServer:
         now = self.clock()
         if self.t0 is None:
             self.t0 = now
+        self.round_frames = []  # (session id, frame bytes) of this round, for the sender
         self._apply_commands(now)
         self._retire(now)
         self._admit(now)
@@ -342,6 +344,7 @@ class SessionServer:
             frame = sv.collect_frame_packed(header)
             t = self.clock()
             self.latencies.append(t - s.request_t)
+            self.round_frames.append((s.id, frame))
             if self.keep_frames:
                 self.frame_log.append((s.id, frame))
             s.last_frame = frame
