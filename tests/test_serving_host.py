@@ -293,3 +293,62 @@ def test_surface_pressure_every_third_frame():
         srv.round()
         c.t += 1 / 30
     assert srv.active[0].solver.cp_frames == [3, 6]
+
+
+# ---- failures stay with their session (server/app.py:115-122, 196-198) ----
+def test_allocation_failure_is_reported_and_others_are_served():
+    c = Clock()
+
+    def factory(s):
+        if s.id == 1:
+            raise MemoryError('out of memory')
+        return FakeSolver(s)
+    srv = serving.SessionServer(device=None, budget_bytes=100, clock=c, solver_factory=factory,
+                                batch_factory=lambda sv, p: FakeBatch(c, 1e12, sv), footprint=lambda s: float(s.n))
+    for i in range(3):
+        srv.submit(_session(i, 4))
+    assert srv.round() == 2
+    assert list(srv.active) == [0, 2] and srv.used == 8
+    assert srv.failed == 1 and srv.errors[0][0] == 1 and 'Could not allocate 4x1x1 grid' in srv.errors[0][1]
+    assert srv.stats()['failed'] == 1
+
+
+def test_frame_failure_retires_only_that_session():
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 4))
+    srv.submit(_session(1, 4))
+    srv.round()
+    bad = srv.active[0].solver
+
+    def boom(p, want_cp):
+        raise RuntimeError('frame kernel failed')
+    bad.launch_frame_packed = boom
+    c.t += 1 / 30
+    assert srv.round() == 1
+    assert list(srv.active) == [1] and srv.used == 4 and srv.failed == 1
+    assert srv.errors == [(0, "solver error: RuntimeError('frame kernel failed')")]
+    c.t += 1 / 30
+    srv.round()
+    assert FakeBatch.log[-1] == (1,)  # rebuilt without the failed session
+    assert srv.active[1].frames == 3
+
+
+def test_one_tunnel_failing_in_a_step_fails_only_its_session():
+    from batch import MemberError
+    c = Clock()
+    srv = _server(c)
+    for i in range(3):
+        srv.submit(_session(i, 2))
+    orig = FakeBatch.step
+
+    def step(self, k):
+        orig(self, k)
+        raise MemberError([(1, RuntimeError('bounded wait gave up'))])
+    FakeBatch.step = step
+    try:
+        assert srv.round() == 2
+    finally:
+        FakeBatch.step = orig
+    assert list(srv.active) == [0, 2] and srv.errors[0][0] == 1
+    assert srv.active[0].frames == 1 and srv.active[2].frames == 1

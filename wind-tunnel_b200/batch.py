@@ -25,6 +25,15 @@ import wtlib as W
 from wtlib import call, ptr
 
 
+class MemberError(RuntimeError):
+    """Some tunnels of a streams-executor step failed (``failed``: [(index, exception)]); every
+    other tunnel was stepped as asked."""
+
+    def __init__(self, failed):
+        super().__init__('; '.join(f'tunnel {i}: {e}' for i, e in failed))
+        self.failed = failed
+
+
 class TunnelBatch:
     def __init__(self, solvers, params, tile=0, stream=None, mode='persistent'):
         if not solvers:
@@ -81,13 +90,20 @@ class TunnelBatch:
         start = torch.cuda.Event()
         start.record(self.stream)
         flags = W.STEP_MAC_ALL_LAST if mac_all_last else 0
-        for s, p, k in zip(self.solvers, self.params, steps):
+        failed = []
+        for j, (s, p, k) in enumerate(zip(self.solvers, self.params, steps)):
             if k <= 0:
                 continue
             s.stream.wait_event(start)
-            call('wt_step', s.gp, s.cur, int(k), float(p['uIn']), float(p['tau']), float(p['smag']), flags, s.sh)
+            try:
+                call('wt_step', s.gp, s.cur, int(k), float(p['uIn']), float(p['tau']), float(p['smag']), flags, s.sh)
+            except W.WtError as e:  # this tunnel only; the others still step
+                failed.append((j, e))
+                continue
             s.cur ^= int(k) & 1
         self._wait_members()
+        if failed:
+            raise MemberError(failed)
 
     def step(self, steps, mac_all_last=True):
         """Advance every tunnel `steps` steps; with the streams executor `steps` may also be one

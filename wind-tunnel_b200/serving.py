@@ -48,6 +48,7 @@ import numpy as np
 import bodies
 import lbm
 import wire
+from batch import MemberError
 
 PAUSED_HZ = 12  # frames per second of a paused session (server/app.py:20)
 
@@ -141,7 +142,8 @@ class SessionServer:
         self.max_active = 0
         self.active_sum = 0
         self.max_queued = 0
-        self.admitted = self.retired = self.abandoned = 0
+        self.admitted = self.retired = self.abandoned = self.failed = 0
+        self.errors = []          # (session id, message) for the sender: the Engine's 'error' JSON
         self._batch = None
         self._batch_key = None
         self._stream = None
@@ -271,7 +273,13 @@ class SessionServer:
             if self.used + need > self.budget:
                 break
             self.queue.pop(0)
-            s.solver = self.solver_factory(s)
+            try:
+                s.solver = self.solver_factory(s)
+            except Exception as e:  # out of memory etc. (server/app.py:115-122)
+                s.solver = None
+                self.failed += 1
+                self.errors.append((s.id, f'Could not allocate {"x".join(map(str, s.dims))} grid: {e}'))
+                continue
             s.bytes = max(need, s.solver.device_bytes())
             s.admitted_t = s.request_t = s.last_t = now
             self.used += s.bytes
@@ -279,6 +287,20 @@ class SessionServer:
             self.active[s.id] = s
             self.admitted += 1
         self.max_active = max(self.max_active, len(self.active))
+
+    def _fail(self, s, err):
+        """A session whose tunnel raised: reported, retired, its memory released; the others
+        go on (the reference's Engine prints a solver error and keeps serving)."""
+        self._invalidate(s)
+        self.active.pop(s.id, None)
+        self.used -= s.bytes
+        try:
+            s.solver.synchronize()
+        except Exception:
+            pass
+        s.solver = None
+        self.failed += 1
+        self.errors.append((s.id, f'solver error: {err!r}'))
 
     def _retire(self, now):
         gone = [s for s in self.active.values() if now - s.arrival >= s.lifetime]
@@ -322,26 +344,41 @@ class SessionServer:
                 self._batch_key = key
                 self.rebuilds += 1
         t_rebuild = self.clock()
+        broken = {}
         if stepping:
             counts = [ks[s.id] for s in stepping]
             started = self._batch.event(timing=True)
-            self._batch.step(counts[0] if len(set(counts)) == 1 else counts)
+            try:
+                self._batch.step(counts[0] if len(set(counts)) == 1 else counts)
+            except MemberError as e:
+                broken.update((stepping[j].id, err) for j, err in e.failed)
             done = self._batch.event(timing=True)
         for s in due:
+            if s.id in broken:
+                continue
             k = ks[s.id]
-            if k:
-                s.solver.wait_event(done)
-                s.solver.advance_particles(k, s.p)
-            s.frame_no += 1
-            s.solver.launch_frame_packed(s.p, self._want_cp(s))
+            try:
+                if k:
+                    s.solver.wait_event(done)
+                    s.solver.advance_particles(k, s.p)
+                s.frame_no += 1
+                s.solver.launch_frame_packed(s.p, self._want_cp(s))
+            except Exception as e:
+                broken[s.id] = e
         t_issue = self.clock()
         for s in due:
+            if s.id in broken:
+                continue
             sv = s.solver
             k = ks[s.id]
             header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=sv.num_verts, forces=None, steps=k,
                           mlups=s.mlups if (self.rate_in_header and s.running) else 0.0, running=s.running)
             t_prev = s.last_t
-            frame = sv.collect_frame_packed(header)
+            try:
+                frame = sv.collect_frame_packed(header)
+            except Exception as e:
+                broken[s.id] = e
+                continue
             t = self.clock()
             self.latencies.append(t - s.request_t)
             self.round_frames.append((s.id, frame))
@@ -361,17 +398,20 @@ class SessionServer:
             else:
                 # the client acknowledges at once and asks again at its next tick
                 s.request_t = max(t, s.request_t + (self.period if s.running else self.paused_period))
+        for s in due:
+            if s.id in broken:
+                self._fail(s, broken[s.id])
         t_end = self.clock()
         if started is not None:  # every frame has been collected, so both events are complete
             self.step_gpu_s += started.elapsed_time(done) / 1e3
-            self.step_cells += sum(s.n * ks[s.id] for s in stepping)
+            self.step_cells += sum(s.n * ks[s.id] for s in stepping if s.id not in broken)
         for name, a, b in (('admit', now, t_admit), ('rebuild', t_admit, t_rebuild), ('issue', t_rebuild, t_issue),
                            ('collect', t_issue, t_end)):
             self.phase[name] += b - a
         self.round_s.append(t_end - now)
         self.rounds += 1
         self.active_sum += len(self.active)
-        return len(due)
+        return len(due) - len(broken)
 
     def stats(self):
         now = self.clock()
@@ -381,7 +421,8 @@ class SessionServer:
         return {'frames': len(self.latencies), 'p50_ms': round(float(np.percentile(lat, 50)), 2),
                 'p99_ms': round(float(np.percentile(lat, 99)), 2), 'max_ms': round(float(lat.max()), 2),
                 'rounds': self.rounds, 'batch_rebuilds': self.rebuilds, 'admitted': self.admitted,
-                'retired': self.retired, 'abandoned': self.abandoned, 'active_end': len(self.active),
+                'retired': self.retired, 'abandoned': self.abandoned, 'failed': self.failed,
+                'active_end': len(self.active),
                 'max_active': self.max_active,
                 'mean_active': round(self.active_sum / max(1, self.rounds), 1), 'queued_end': len(self.queue),
                 'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
