@@ -473,7 +473,7 @@ def main():
         serving_out = {}
         for prec in ('fp32', 'fp16'):
             serving_out[prec] = serving.simulate(duration=args.serving, precision=prec, device=f'cuda:{local_rank}',
-                                                 mask_set=ms)
+                                                 mask_set=ms, warmup_s=3.0)
             torch.cuda.empty_cache()
     cpu = None
     if rank == 0 and not args.no_cpu:

@@ -501,13 +501,14 @@ class Arrivals:
 
 def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='fp32', seed=5, device='cuda:0',
              particles=5000, warm_start=True, tile=0, steps_per_frame=10, fps=30.0, mask_set=None, keep=None,
-             before_window=None, latencies_out=None, server_factory=None):
+             before_window=None, latencies_out=None, server_factory=None, warmup_s=0.0):
     """Config 5 in wall-clock time: Poisson arrivals at `rate` per second for `duration`
     seconds, each session requesting `fps` frames per second of its particles, one slice and
     Cd/Cl, admitted against `budget` bytes. With warm_start the run begins from the arrival
     process's stationary population (Poisson with mean rate x mean_life sessions; lifetimes
     are memoryless, so their residual lifetimes are exponential with the same mean), so the
-    window measures the steady state; the set-up of those sessions is not timed.
+    window measures the steady state; the set-up of those sessions is not timed. ``warmup_s``
+    seconds of rounds over those sessions (no arrivals, not timed) come before the window.
 
     For one GPU of several (placement.py): ``keep(session, t)`` is asked about every session
     of the arrival stream, t its arrival in seconds from the start of the window (0 for the
@@ -529,6 +530,10 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
             offer(gen.session(start), 0.0)
         srv._admit(start)
         srv.round()  # the stationary sessions have been running: one round builds their batch
+        t_warm = time.perf_counter()
+        while time.perf_counter() - t_warm < warmup_s:
+            if srv.round() == 0:
+                time.sleep(0.0005)
     setup_s = time.perf_counter() - start
     if before_window is not None:
         before_window()
@@ -555,7 +560,7 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     out = srv.stats()
     out.update(precision=precision, duration_s=duration, arrival_rate=rate, mean_lifetime_s=mean_life,
                budget_gb=budget / 1e9, warm_start=warm_start, steps_per_frame=steps_per_frame, fps=fps,
-               particles=particles, setup_s=round(setup_s, 1))
+               particles=particles, setup_s=round(setup_s, 1), warmup_s=warmup_s)
     if latencies_out is not None:
         latencies_out.extend(srv.latencies)
     srv.close()
@@ -572,11 +577,12 @@ def main(argv=None):
     ap.add_argument('--steps-per-frame', type=int, default=10)
     ap.add_argument('--tile', type=int, default=0)
     ap.add_argument('--seed', type=int, default=5)
+    ap.add_argument('--warmup', type=float, default=3.0, help='untimed seconds of rounds before the window')
     a = ap.parse_args(argv)
     ms = masks()
     for prec in a.precision:
         r = simulate(a.duration, a.rate, a.mean_life, a.budget_gb * 1e9, prec, a.seed, tile=a.tile,
-                     steps_per_frame=a.steps_per_frame, mask_set=ms)
+                     steps_per_frame=a.steps_per_frame, mask_set=ms, warmup_s=a.warmup)
         print(json.dumps(r), flush=True)
 
 
