@@ -239,6 +239,35 @@ def test_random_obstacles_match_oracle(oracle_mod, prec_name, oprec, shift, dims
     np.testing.assert_allclose(s.mass(), L.mass(), rtol=1e-13)
 
 
+def test_config1_sphere_2000_steps_matches_oracle(oracle_mod):
+    """The reference's CPU-runnable workload at its full size: 128x64x64, sphere r = 8 at
+    (40, 32, 32), no-slip floor, u = 0.05, nu = 0.002, 2000 steps from equilibrium. Populations
+    and mac bit for bit every 50 steps; the drag and lift (fp64 sums of all links, and without
+    the floor's) and Cd/Cl on the sphere's frontal area against the oracle's at every check."""
+    import os
+    import bodies
+    dims, solid, p = bodies.config1()
+    oracle_mod.set_threads(os.cpu_count() or 1)
+    s = _solver(dict(dims=np.array(dims), solid=solid), 'fp32')
+    s.reset(p['uIn'])
+    L = oracle_mod.Lattice(dims, 0)
+    L.solid[:] = solid
+    L.reset(p['uIn'])
+    frontal = bodies.areas(solid, dims)[0]
+    q = 0.5 * p['uIn'] ** 2 * frontal
+    for k in range(40):
+        s.step(50, p)
+        L.step(50, p['uIn'], p['tau'], p['smag'])
+        s.synchronize()
+        assert np.array_equal(s.f[s.cur].cpu().numpy(), L.f[L.cur]), f'populations after {50 * (k + 1)} steps'
+        assert np.array_equal(s.mac[s.cur].cpu().numpy(), L.mac), f'mac after {50 * (k + 1)} steps'
+        _, d64, b64 = L.forces()
+        f6 = s.forces6()
+        np.testing.assert_allclose(f6[:3], d64, rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(f6[3:], b64, rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose([f6[3] / q, f6[4] / q], [b64[0] / q, b64[1] / q], rtol=1e-12, atol=1e-14)
+
+
 def _degenerate(name):
     """Grids at and near the smallest the library accepts, and masks with nothing to do."""
     if name == 'min_4x3x3_fluid':
