@@ -268,6 +268,31 @@ def test_config1_sphere_2000_steps_matches_oracle(oracle_mod):
         np.testing.assert_allclose([f6[3] / q, f6[4] / q], [b64[0] / q, b64[1] / q], rtol=1e-12, atol=1e-14)
 
 
+@pytest.mark.parametrize('prec_name,oprec', [('fp32', 0), ('fp16', 1)])
+def test_benchmark_workload_full_size_matches_oracle(oracle_mod, prec_name, oprec):
+    """The 512x256x256 benchmark body (33.5M cells, the largest configuration) for 6 steps, the
+    last writing mac for every cell: populations, mac, forces and mass against the oracle."""
+    import os
+    import bodies
+    dims, solid, p = bodies.config2()
+    oracle_mod.set_threads(os.cpu_count() or 1)
+    s = _solver(dict(dims=np.array(dims), solid=solid), prec_name)
+    s.reset(p['uIn'])
+    L = oracle_mod.Lattice(dims, oprec, shift_u=float(s.grid.shift_u))
+    L.solid[:] = solid
+    L.reset(p['uIn'])
+    s.step(6, p)
+    L.step(6, p['uIn'], p['tau'], p['smag'])
+    s.synchronize()
+    assert np.array_equal(s.f[s.cur].cpu().numpy(), L.f[L.cur])
+    assert np.array_equal(s.mac[s.cur].cpu().numpy(), L.mac)
+    _, d64, b64 = L.forces()
+    f6 = s.forces6()
+    np.testing.assert_allclose(f6[:3], d64, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(f6[3:], b64, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(s.mass(), L.mass(), rtol=1e-13)
+
+
 def _degenerate(name):
     """Grids at and near the smallest the library accepts, and masks with nothing to do."""
     if name == 'min_4x3x3_fluid':
