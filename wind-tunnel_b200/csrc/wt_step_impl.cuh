@@ -771,11 +771,15 @@ template <int PREC>
 __device__ __forceinline__ void pair_load(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                           int32_t idx0, PairRaw<typename Prec<PREC>::S>& r) {
     using S = typename Prec<PREC>::S;
-    // one per-thread base; the per-population offsets are the same for every thread
+    // float and double: each population from its own pull base (a kernel parameter) plus the
+    // cell index; half width: one per-thread base plus offsets that are the same for every
+    // thread (the faster form for each, measured)
     const S* fb = a.fin + idx0;
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        const S* p = fb + ((int64_t)i * a.n - (cx(i) + cy(i) * (int64_t)a.nx + cz(i) * (int64_t)a.nxy));
+        const S* p = sizeof(S) >= 4
+                         ? a.src[i] + idx0
+                         : fb + ((int64_t)i * a.n - (cx(i) + cy(i) * (int64_t)a.nx + cz(i) * (int64_t)a.nxy));
         r.v[i] = vload<S, 2>(p + cx(i));  // aligned: the shift cancels
         if constexpr (cx(i) > 0) r.e[i] = p[0];
         if constexpr (cx(i) < 0) r.e[i] = p[1];
@@ -863,7 +867,7 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
     if (!sol0 && !sol1) {
         unroll<0, Q>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            store_cells<P, FAST, 2, i>(a, ob + (int64_t)i * a.n, f);
+            store_cells<P, FAST, 2, i>(a, sizeof(typename P::S) >= 4 ? a.dst[i] + idx0 : ob + (int64_t)i * a.n, f);
         });
     } else {
         const int32_t k = sol0 ? 1 : 0;  // the one fluid cell of the pair (selects, no indexing)
