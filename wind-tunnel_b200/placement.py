@@ -127,6 +127,7 @@ def main(argv=None):
     ap.add_argument('--precision', nargs='+', default=['fp32', 'fp16'])
     ap.add_argument('--steps-per-frame', type=int, default=10)
     ap.add_argument('--seed', type=int, default=5)
+    ap.add_argument('--warmup', type=float, default=3.0, help='untimed seconds of rounds before the window')
     a = ap.parse_args(argv)
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -140,7 +141,8 @@ def main(argv=None):
         barrier = dist.barrier if world > 1 else None
         out, lat = simulate_rank(rank, world, precision=prec, budget=a.budget_gb * 1e9, barrier=barrier,
                                  duration=a.duration, rate=a.rate * world, mean_life=a.mean_life, seed=a.seed,
-                                 device=f'cuda:{local}', steps_per_frame=a.steps_per_frame, mask_set=ms)
+                                 device=f'cuda:{local}', steps_per_frame=a.steps_per_frame, mask_set=ms,
+                                 warmup_s=a.warmup)
         if world > 1:
             gathered = [None] * world
             dist.all_gather_object(gathered, (out, lat))
