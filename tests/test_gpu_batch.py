@@ -3,7 +3,6 @@ the same tunnel stepped alone with wt_step, for direct steps, odd step counts an
 replays."""
 import numpy as np
 import pytest
-import torch
 
 pytestmark = pytest.mark.gpu
 

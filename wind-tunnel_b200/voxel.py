@@ -8,7 +8,7 @@ import numpy as np
 import torch
 
 import wtlib as W
-from wtlib import call, ptr
+from wtlib import ptr
 
 
 def voxelize(tris, dims, ground=True, device='cuda:0', stream=None):
