@@ -352,3 +352,16 @@ def test_one_tunnel_failing_in_a_step_fails_only_its_session():
         FakeBatch.step = orig
     assert list(srv.active) == [0, 2] and srv.errors[0][0] == 1
     assert srv.active[0].frames == 1 and srv.active[2].frames == 1
+
+
+def test_a_malformed_command_fails_alone():
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 4))
+    srv.round()
+    srv.command(0, {'type': 'solid', 'dims': [4, 1, 1]}, b'not gzip')
+    srv.command(0, {'type': 'params', 'tau': 0.55})
+    c.t += 1 / 30
+    assert srv.round() == 1
+    assert srv.errors[0][0] == 0 and srv.errors[0][1].startswith('command failed:')
+    assert srv.active[0].p['tau'] == 0.55  # the next command still ran

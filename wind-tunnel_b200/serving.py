@@ -198,7 +198,10 @@ class SessionServer:
                 s = next((q for q in self.queue if q.id == sid), None)
             if s is None:
                 continue  # gone, or never here: the reference ignores commands without a solver
-            self._apply(s, msg, payload, now)
+            try:
+                self._apply(s, msg, payload, now)
+            except Exception as e:  # a bad message fails alone (the Engine reports it, server/app.py:160-161)
+                self.errors.append((sid, f'command failed: {e!r}'))
 
     def _apply(self, s, msg, payload, now):
         t = msg.get('type')
