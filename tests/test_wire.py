@@ -54,3 +54,38 @@ def test_layout_frame_equals_pack(k):
         buf[lay.offsets[name]:lay.offsets[name] + raw.size] = raw
     assert lay.forces_offset % 8 == 0 and lay.total_bytes == lay.payload_bytes + 48
     assert lay.frame(header, buf) == ref
+
+
+# ---- client uploads (web/js/net.js:9-16, 85-92 framing; server/app.py:138-148, 218-222 checks) ----
+def test_upload_framing_round_trip():
+    import gzip
+    import struct
+    header = {'type': 'solid', 'dims': [4, 3, 3]}
+    body = bytes(range(36))
+    msg = wire.encode_upload(header, body)
+    hl = struct.unpack_from('<I', msg, 0)[0]
+    assert msg[4:4 + hl].decode() == '{"type":"solid","dims":[4,3,3]}'
+    h, payload = wire.decode_upload(msg)
+    assert h == header and gzip.decompress(payload) == body
+
+
+def test_upload_arrays_accepts_what_the_engine_accepts():
+    mask = (np.arange(36) % 3).astype(np.uint8)
+    h, p = wire.decode_upload(wire.encode_upload({'type': 'solid', 'dims': [4, 3, 3]}, mask.tobytes()))
+    kind, arr = wire.upload_arrays(h, p, (4, 3, 3))
+    assert kind == 'solid' and np.array_equal(arr, mask)
+    vn = np.arange(2 * 6, dtype=np.float32)
+    h, p = wire.decode_upload(wire.encode_upload({'type': 'surface', 'numVerts': 2}, vn.tobytes()))
+    kind, verts, norms = wire.upload_arrays(h, p, (4, 3, 3))
+    assert kind == 'surface'
+    assert np.array_equal(verts, vn[:6].reshape(2, 3)) and np.array_equal(norms, vn[6:].reshape(2, 3))
+
+
+def test_upload_arrays_ignores_what_the_engine_ignores():
+    mask = np.zeros(36, np.uint8)
+    for header, body, dims in [({'type': 'solid', 'dims': [4, 3, 4]}, mask, (4, 3, 3)),        # another grid
+                               ({'type': 'solid', 'dims': [4, 3, 3]}, mask[:35], (4, 3, 3)),   # short mask
+                               ({'type': 'surface', 'numVerts': 3}, np.zeros(12, np.float32), (4, 3, 3)),
+                               ({'type': 'unknown'}, mask, (4, 3, 3))]:
+        h, p = wire.decode_upload(wire.encode_upload(header, body.tobytes()))
+        assert wire.upload_arrays(h, p, dims) is None

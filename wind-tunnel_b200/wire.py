@@ -96,7 +96,7 @@ def encode_upload(header, payload):
     """A client's binary message: [u32 LE header length][JSON header][gzip of payload], as
     the browser's frameBytes(header, await gzip(bytes)) builds it."""
     import gzip
-    hb = json.dumps(header).encode()
+    hb = json.dumps(header, separators=(',', ':')).encode()  # JSON.stringify's compact form
     return struct.pack('<I', len(hb)) + hb + gzip.compress(bytes(payload))
 
 
