@@ -365,3 +365,18 @@ def test_a_malformed_command_fails_alone():
     assert srv.round() == 1
     assert srv.errors[0][0] == 0 and srv.errors[0][1].startswith('command failed:')
     assert srv.active[0].p['tau'] == 0.55  # the next command still ran
+
+
+def test_disconnect_retires_or_dequeues():
+    c = Clock()
+    srv = _server(c, budget=4)
+    srv.submit(_session(0, 4))
+    srv.submit(_session(1, 4))
+    srv.round()
+    assert list(srv.active) == [0] and [q.id for q in srv.queue] == [1]
+    srv.disconnect(1)  # still waiting: leaves the queue
+    srv.disconnect(0)  # admitted: retired, memory released
+    c.t += 1 / 30
+    assert srv.round() == 0
+    assert not srv.active and not srv.queue and srv.used == 0
+    assert srv.retired == 1 and srv.abandoned == 1

@@ -184,6 +184,11 @@ class SessionServer:
             raise ValueError("a resolution change is a new session; submit one")
         self._cmds.append((sid, dict(msg), payload))
 
+    def disconnect(self, sid):
+        """The session's client has gone (its WebSocket closed): at the next round an admitted
+        session is retired and its memory released, and one still waiting leaves the queue."""
+        self._cmds.append((sid, None, None))
+
     def _invalidate(self, s):
         # a batched tunnel's parameters, buffers or mask changed: rebuild the batch
         if self._batch is not None and self._batch_key is not None and s.id in self._batch_key:
@@ -198,6 +203,9 @@ class SessionServer:
                 s = next((q for q in self.queue if q.id == sid), None)
             if s is None:
                 continue  # gone, or never here: the reference ignores commands without a solver
+            if msg is None:  # disconnected: the lifetime ends now (retired or abandoned below)
+                s.lifetime = min(s.lifetime, now - s.arrival)
+                continue
             try:
                 self._apply(s, msg, payload, now)
             except Exception as e:  # a bad message fails alone (the Engine reports it, server/app.py:160-161)
