@@ -29,7 +29,10 @@ owns a tunnel on one GPU:
   session steps its own 'steps' per frame; surface pressure comes every third frame when
   'cp' is on (server/app.py:177-178). With ``pacing='client'`` a session's next frame waits for
   its client's 'ready', as in the reference; the default ``'fps'`` stands in for clients that
-  acknowledge at once and ask again at their next 1/fps tick.
+  acknowledge at once and ask again at their next 1/fps tick. ``disconnect(session)`` ends a
+  session whose client has gone.
+* **Failures.** A solver that cannot be created, or a session whose step, particles, frame or
+  command raises, fails alone: it is reported in ``errors`` and the others are served.
 * **Latency.** A frame's latency runs from its request to the moment its bytes are on the
   host. ``stats()`` gives p50/p99 over all frames, admitted/retired/abandoned/queued counts,
   the peak and end memory in use, and the aggregate lattice-update rate over the window.
