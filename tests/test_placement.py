@@ -14,8 +14,12 @@ import serving
 
 
 class _S:
+    count = 0
+
     def __init__(self, n, lifetime=1e9):
         self.n, self.lifetime = n, lifetime
+        self.id = _S.count
+        _S.count += 1
 
 
 def test_least_connected_cells_with_ties_to_lower_index():
@@ -50,6 +54,20 @@ def test_departures_free_the_gpu():
     assert p.cells == [20, 30]
     with pytest.raises(ValueError):
         p.place(_S(1), 0.5)
+
+
+def test_departures_reported_by_a_front_end():
+    """Unknown lifetimes: sessions stay until leave() reports their client gone."""
+    p = placement.Placer(2, 100, footprint=lambda s: s.n)
+    a, b = _S(40, lifetime=float('inf')), _S(10, lifetime=float('inf'))
+    assert p.place(a, 0.0) == 0 and p.place(b, 0.0) == 1
+    assert p.place(_S(5, lifetime=float('inf')), 50.0) == 1  # a is still connected
+    p.leave(a, 60.0)
+    assert p.cells == [0, 15] and p.bytes == [0, 15]
+    p.leave(a, 61.0)  # already gone: ignored
+    assert p.place(_S(5, lifetime=float('inf')), 62.0) == 0
+    with pytest.raises(ValueError):
+        p.leave(b, 10.0)
 
 
 def test_merge_pools_latencies_and_sums_counts():

@@ -48,15 +48,33 @@ class Placer:
         self.placed = [0] * self.gpus      # sessions placed per GPU, all time
         self.placed_cells = [0] * self.gpus
         self.assignment = []               # the GPU of every session placed, in arrival order
-        self._ends = []                    # (departure, sequence, gpu, cells, bytes)
+        self._ends = []                    # (departure, sequence, session id) of known lifetimes
+        self._live = {}                    # session id -> (gpu, cells, bytes) while connected
         self._seq = 0
         self._last_t = float('-inf')
 
+    def _drop(self, sid):
+        g, n, b = self._live.pop(sid)
+        self.cells[g] -= n
+        self.bytes[g] -= b
+
     def _depart(self, t):
         while self._ends and self._ends[0][0] <= t:
-            _, _, g, n, b = heapq.heappop(self._ends)
-            self.cells[g] -= n
-            self.bytes[g] -= b
+            sid = heapq.heappop(self._ends)[2]
+            if sid in self._live:
+                self._drop(sid)
+
+    def leave(self, session, t):
+        """The session's client disconnected at t (a front end that does not know lifetimes
+        reports departures this way; every rank must see the same departures in the same order
+        as the arrivals). Unknown or already departed sessions are ignored."""
+        t = float(t)
+        if t < self._last_t:
+            raise ValueError('departures must be reported in time order with the arrivals')
+        self._last_t = t
+        self._depart(t)
+        if session.id in self._live:
+            self._drop(session.id)
 
     def place(self, session, t):
         t = float(t)
@@ -74,7 +92,9 @@ class Placer:
         self.bytes[g] += need
         self.placed[g] += 1
         self.placed_cells[g] += session.n
-        heapq.heappush(self._ends, (t + session.lifetime, self._seq, g, session.n, need))
+        self._live[session.id] = (g, session.n, need)
+        if session.lifetime != float('inf'):
+            heapq.heappush(self._ends, (t + session.lifetime, self._seq, session.id))
         self._seq += 1
         self.assignment.append(g)
         return g
