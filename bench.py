@@ -17,10 +17,16 @@ reset, then K frames each with its outputs read back to pinned host memory). Pop
 N > 1 runs independent replicas, one tunnel per GPU ("replicas only": independent
 tunnels never exchange data); time is the max over ranks.
 
-At N = 1 the line also carries `serving`: the config-5 serving loop (Poisson sessions of
+The line also carries, for the fp32 default run: `roofline` (the fused step alone against the
+HBM peak, with a 2 GiB device copy timed in the same run beside it), `cpu_baseline` (the
+oracle on the host cores), `precision_variants` (fp32 fast, fp16 and bf16 shifted storage,
+fp16 exact), `accuracy_vs_fp64` (a chaotic and a laminar regime against an fp64 run),
+`batching` (the 24-tunnel batch of config 4 under both batch executors, one tunnel re-run
+alone and compared bit for bit), and `voxelize` (the server-side voxeliser on the benchmark
+body). At N = 1 it carries `serving`: the config-5 serving loop (Poisson sessions of
 0.5-33.5M cells under a 160 GB budget, 30 frames/s requested per session) run from its
-stationary population for `--serving` seconds per storage precision, with p50/p99 frame
-latency, admitted sessions and aggregate GLUPS.
+stationary population, after 3 s of untimed rounds, for `--serving` seconds per storage
+precision, with p50/p99 frame latency, admitted sessions and aggregate GLUPS.
 """
 import argparse
 import json
