@@ -380,3 +380,9 @@ def test_disconnect_retires_or_dequeues():
     assert srv.round() == 0
     assert not srv.active and not srv.queue and srv.used == 0
     assert srv.retired == 1 and srv.abandoned == 1
+
+
+def test_fits_is_the_admission_bound():
+    c = Clock()
+    srv = _server(c, budget=10)  # the fake footprint is one byte per cell
+    assert srv.fits((10, 1, 1)) and not srv.fits((11, 1, 1))

@@ -187,6 +187,13 @@ class SessionServer:
             raise ValueError("a resolution change is a new session; submit one")
         self._cmds.append((sid, dict(msg), payload))
 
+    def fits(self, dims, particles=5000):
+        """Whether a session of this grid can ever be admitted: its footprint within the HBM
+        budget. The Engine's fits() (server/app.py:71-75) asks the same of a resolution before
+        it builds a Solver, and answers 'does not fit on this device' otherwise."""
+        return self.footprint(Session(-1, dims, None, dict(uIn=0.05, tau=0.51, smag=0.16), 0.0,
+                                      particles=particles, frontal=1)) <= self.budget
+
     def disconnect(self, sid):
         """The session's client has gone (its WebSocket closed): at the next round an admitted
         session is retired and its memory released, and one still waiting leaves the queue."""
