@@ -386,3 +386,24 @@ def test_fits_is_the_admission_bound():
     c = Clock()
     srv = _server(c, budget=10)  # the fake footprint is one byte per cell
     assert srv.fits((10, 1, 1)) and not srv.fits((11, 1, 1))
+
+
+def test_command_arriving_during_a_drain_waits_for_the_next_round():
+    c = Clock()
+    srv = _server(c)
+    srv.submit(_session(0, 4))
+    srv.round()
+    sv = srv.active[0].solver
+    orig = sv.reset
+
+    def reset_and_more(uin):  # another thread's command lands while this round drains
+        orig(uin)
+        srv.command(0, {'type': 'respawn'})
+    sv.reset = reset_and_more
+    srv.command(0, {'type': 'reset'})
+    c.t += 1 / 30
+    srv.round()
+    assert [k for k, _ in sv.calls] == ['reset']
+    c.t += 1 / 30
+    srv.round()
+    assert [k for k, _ in sv.calls] == ['reset', 'set_particles']

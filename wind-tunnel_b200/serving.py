@@ -42,6 +42,7 @@ every session is due in every round, frames come as fast as the GPU allows, and 
 latency equals the round time: steps_per_frame x cells in service / throughput.
 """
 import argparse
+import collections
 import heapq
 import json
 import time
@@ -130,7 +131,10 @@ class SessionServer:
         self.pacing = pacing
         self.paused_period = 1.0 / paused_hz
         self.rate_in_header = rate_in_header
-        self._cmds = []           # (session id, message, payload) in arrival order
+        # (session id, message, payload) in arrival order; a deque, so the front end's threads
+        # can append while the serving thread drains (the reference's handlers feed its Engine
+        # through a queue the same way, server/app.py:212-222)
+        self._cmds = collections.deque()
         self.round_frames = []    # (session id, frame bytes) produced by the latest round
         self.active = {}          # id -> Session, in admission order
         self.queue = []           # FIFO of sessions waiting for memory
@@ -182,7 +186,9 @@ class SessionServer:
         halves wire.decode_upload returns). Commands run in arrival order at the start of the
         next round, as the reference's Engine drains its queue before it steps. A session still
         waiting for memory keeps its parameters and uploads for when it is admitted. A
-        resolution change ('grid') is a new session: its footprint goes through admission."""
+        resolution change ('grid') is a new session: its footprint goes through admission.
+        command() and disconnect() may be called from other threads (a WebSocket front end's
+        handlers) while the serving thread runs rounds."""
         if msg.get('type') == 'grid':
             raise ValueError("a resolution change is a new session; submit one")
         self._cmds.append((sid, dict(msg), payload))
@@ -206,8 +212,8 @@ class SessionServer:
             self._batch, self._batch_key = None, None
 
     def _apply_commands(self, now):
-        cmds, self._cmds = self._cmds, []
-        for sid, msg, payload in cmds:
+        for _ in range(len(self._cmds)):  # those queued before this round; later ones wait
+            sid, msg, payload = self._cmds.popleft()
             s = self.active.get(sid)
             if s is None:
                 s = next((q for q in self.queue if q.id == sid), None)
