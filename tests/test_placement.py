@@ -73,10 +73,10 @@ def test_departures_reported_by_a_front_end():
 def test_merge_pools_latencies_and_sums_counts():
     keys = dict(p50_ms=0, p99_ms=0, abandoned=0, retired=1, mean_active=2.5, glups=1.5, step_glups_device=2.0,
                 peak_used_gb=3.0)
-    a = dict(keys, frames=3, admitted=2, placed=2)
-    b = dict(keys, frames=1, admitted=1, placed=1, peak_used_gb=5.0)
+    a = dict(keys, frames=3, admitted=2, placed=2, failed=1)
+    b = dict(keys, frames=1, admitted=1, placed=1, peak_used_gb=5.0, failed=0)
     m = placement.merge([a, b], [[0.001, 0.002, 0.003], [0.1]])
-    assert m['frames'] == 4 and m['admitted'] == 3 and m['gpus'] == 2
+    assert m['frames'] == 4 and m['admitted'] == 3 and m['gpus'] == 2 and m['failed'] == 1
     assert m['glups'] == 3.0 and m['step_glups_device'] == 4.0 and m['mean_active'] == 5.0
     assert m['peak_used_gb_max'] == 5.0
     assert m['p50_ms'] == pytest.approx(np.percentile([1, 2, 3, 100], 50))

@@ -112,7 +112,7 @@ def merge(stats, latencies):
             'p50_ms': round(float(np.percentile(lat, 50)), 2), 'p99_ms': round(float(np.percentile(lat, 99)), 2),
             'max_ms': round(float(lat.max()), 2),
             'admitted': int(total('admitted')), 'abandoned': int(total('abandoned')),
-            'retired': int(total('retired')),
+            'retired': int(total('retired')), 'failed': int(sum(s.get('failed', 0) for s in stats)),
             'mean_active': round(float(total('mean_active')), 1),
             'glups': round(float(total('glups')), 3),
             'step_glups_device': round(float(total('step_glups_device')), 3),
