@@ -9,105 +9,13 @@
 //   faces -- work items {tunnel, first face index} of FACE_BLOCK * ITEM_SUB face cells each.
 // Each CTA copies the descriptor of its current item into shared memory, so the kernel body
 // is the single-tunnel one (bulk_cells / face_cell of wt_step_impl.cuh) and every tunnel
-// gives bit-identical results alone or in a batch.
+// gives bit-identical results alone or in a batch. The kernels (k_batch_bulk, k_batch_faces)
+// are instantiated per precision in wt_kernels_<prec>.cu; this file is the host side.
 #include <cstring>
 #include <vector>
 
 #include "wt_step_impl.cuh"
-
-namespace wt {
-
-// A work item is ITEM_SUB sub-tiles: BLOCK * V * ITEM_SUB cells of one tunnel (bulk) or
-// FACE_BLOCK * ITEM_SUB face cells (faces); the descriptor copy and its two barriers are
-// paid once per item.
-constexpr int ITEM_SUB = 16;
-constexpr int FACE_BLOCK = 256;
-
-struct BatchArgs {
-    const void* desc;  // StepArgs<S, T>[count][2][2] of the batch's precision
-    const int2* bulk;
-    const int2* faces;
-    int32_t n_bulk, n_faces;
-    int32_t parity, mac_all;
-};
-
-// one descriptor into shared memory (all threads; two barriers around the use)
-template <class A>
-__device__ __forceinline__ void copy_desc(A* dst, const A* src) {
-    static_assert(sizeof(A) % 4 == 0, "descriptor size");
-    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
-    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
-    for (int k = threadIdx.x; k < (int)(sizeof(A) / 4); k += blockDim.x) d[k] = s[k];
-}
-
-template <int PREC, bool FAST, int V, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_batch_bulk(const BatchArgs b) {
-    using A = StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>;
-    __shared__ __align__(16) A a;
-#pragma unroll 1
-    for (int32_t w = blockIdx.x; w < b.n_bulk; w += gridDim.x) {
-        const int2 item = b.bulk[w];
-        copy_desc(&a, static_cast<const A*>(b.desc) + item.x * 4 + b.parity * 2 + b.mac_all);
-        __syncthreads();
-        // SUB consecutive sub-tiles of BLOCK * V cells, no barrier between them
-#pragma unroll 1
-        for (int sub = 0; sub < ITEM_SUB; ++sub) {
-            const int32_t idx0 = item.y + (sub * BLOCK + (int32_t)threadIdx.x) * V;
-            bulk_cells<PREC, FAST, V>(a, idx0, idx0 < a.n);
-        }
-        __syncthreads();
-    }
-}
-
-template <int PREC>
-__global__ void __launch_bounds__(FACE_BLOCK) k_batch_faces(const BatchArgs b) {
-    using A = StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>;
-    __shared__ __align__(16) A a;
-#pragma unroll 1
-    for (int32_t w = blockIdx.x; w < b.n_faces; w += gridDim.x) {
-        const int2 item = b.faces[w];
-        copy_desc(&a, static_cast<const A*>(b.desc) + item.x * 4 + b.parity * 2 + b.mac_all);
-        __syncthreads();
-#pragma unroll 1
-        for (int sub = 0; sub < ITEM_SUB; ++sub) face_cell<PREC>(a, item.y + sub * FACE_BLOCK + (int32_t)threadIdx.x);
-        __syncthreads();
-    }
-}
-
-struct BatchVariant {
-    int id, v, block, minb;
-    void (*bulk)(const void* args, int grid, cudaStream_t st);
-    void (*faces)(const void* args, int grid, cudaStream_t st);
-};
-
-template <int PREC, bool FAST, int V, int BLOCK, int MINB>
-static void launch_batch_bulk(const void* args, int grid, cudaStream_t st) {
-    k_batch_bulk<PREC, FAST, V, BLOCK, MINB><<<grid, BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
-}
-template <int PREC>
-static void launch_batch_faces(const void* args, int grid, cudaStream_t st) {
-    k_batch_faces<PREC><<<grid, FACE_BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
-}
-
-// the direct-load tile shapes of wt_step, same ids
-#define WT_BATCH_VARIANTS(PREC, FAST)                                                                        \
-    {1, 1, 256, 4, launch_batch_bulk<PREC, FAST, 1, 256, 4>, launch_batch_faces<PREC>},                      \
-    {2, 1, 128, 8, launch_batch_bulk<PREC, FAST, 1, 128, 8>, launch_batch_faces<PREC>},                      \
-    {3, 2, 128, 6, launch_batch_bulk<PREC, FAST, 2, 128, 6>, launch_batch_faces<PREC>},                      \
-    {4, 2, 128, 4, launch_batch_bulk<PREC, FAST, 2, 128, 4>, launch_batch_faces<PREC>},                      \
-    {5, 4, 128, 4, launch_batch_bulk<PREC, FAST, 4, 128, 4>, launch_batch_faces<PREC>},                      \
-    {7, 2, 256, 3, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>},                      \
-    {18, 2, 128, 8, launch_batch_bulk<PREC, FAST, 2, 128, 8>, launch_batch_faces<PREC>}
-
-template <int PREC, bool FAST>
-static const BatchVariant* batch_variant(int id) {
-    static const BatchVariant table[] = {WT_BATCH_VARIANTS(PREC, FAST)};
-    for (const auto& v : table)
-        if (v.id == id) return &v;
-    return nullptr;
-}
-
-}  // namespace wt
+#include "wt_variants.cuh"
 
 using namespace wt;
 
@@ -209,11 +117,6 @@ void fill_desc(const wt_grid& g, int32_t cur0, double uin, double tau, double sm
     std::memcpy(out, &a, sizeof(a));
 }
 
-template <int PREC>
-const BatchVariant* pick(int32_t collision, int id) {
-    return collision == WT_COLLIDE_FAST ? batch_variant<PREC, true>(id) : batch_variant<PREC, false>(id);
-}
-
 int launch_steps(wt_batch* b, int32_t steps, int32_t flags, cudaStream_t st) {
     for (int32_t s = 0; s < steps; ++s) {
         const int parity = (b->base + s) & 1;
@@ -258,10 +161,10 @@ extern "C" int wt_batch_create(const wt_grid* grids, int32_t count, const double
     if (!id) return wt_set_error(WT_ERR_ARG, "wt_batch: tile %d has no batched form", tile);
     const BatchVariant* var = nullptr;
     switch (prec) {
-        case WT_F32: var = pick<WT_F32>(coll, id); break;
-        case WT_F16: var = pick<WT_F16>(coll, id); break;
-        case WT_BF16: var = pick<WT_BF16>(coll, id); break;
-        case WT_F64: var = pick<WT_F64>(coll, id); break;
+        case WT_F32: var = batch_variant<WT_F32>(coll == WT_COLLIDE_FAST, id); break;
+        case WT_F16: var = batch_variant<WT_F16>(coll == WT_COLLIDE_FAST, id); break;
+        case WT_BF16: var = batch_variant<WT_BF16>(coll == WT_COLLIDE_FAST, id); break;
+        case WT_F64: var = batch_variant<WT_F64>(coll == WT_COLLIDE_FAST, id); break;
         default: return wt_set_error(WT_ERR_ARG, "wt_batch_create: unknown precision %d", prec);
     }
     if (!var) return wt_set_error(WT_ERR_ARG, "wt_batch_create: no batched kernel for tile %d", id);

@@ -1,0 +1,5 @@
+// Step and batch kernels for bf16 population storage (one translation unit per storage
+// precision, so the build compiles the four in parallel).
+#include "wt_kernels.cuh"
+
+WT_INSTANTIATE(WT_BF16)

@@ -1,147 +1,6 @@
-// Single-tunnel step entry point (wt_step) and the tile-variant table of the step kernels.
-// The kernels themselves are in wt_step_impl.cuh (shared with the batched form, wt_batch.cu).
-#include "wt_step_impl.cuh"
-
-namespace wt {
-
-// Tile variants of the step kernel. Direct-load forms (kind 0): cells per thread (V),
-// threads per block, minimum resident blocks per SM (bounds registers). Streaming forms
-// (kind 1): chunk length L, pipeline stages NS, threads per block, blocks per SM.
-// wt_grid.tile selects one (0 = the default for the precision); autotune.py times them.
-struct StepVariant {
-    int id, kind, v, block, minb, chunk, stages;
-    int (*launch)(const void* args, int32_t n, cudaStream_t st);
-};
-
-
-template <int PREC, bool FAST, int V, int BLOCK, int MINB>
-static int launch_bulk(const void* args, int32_t n, cudaStream_t st) {
-    using P = Prec<PREC>;
-    const auto& a = *static_cast<const StepArgs<typename P::S, typename P::T>*>(args);
-    const int32_t nthreads = n / V;
-    k_step_bulk<PREC, FAST, V, BLOCK, MINB><<<(unsigned)((nthreads + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
-    return WT_OK;
-}
-
-template <int PREC, bool FAST, int L, int NS, int THREADS, int MINB, int CPT>
-static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
-    using P = Prec<PREC>;
-    using LY = StreamLayout<typename P::S, L>;
-    constexpr int SMEM = NS * LY::STAGE_BYTES + 2 * NS * 8;
-    if (SMEM > 227 * 1024) return wt_set_error(WT_ERR_ARG, "streaming tile needs %d bytes of shared memory", SMEM);
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(k_step_stream<PREC, FAST, L, NS, THREADS, MINB, CPT>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
-            return wt_cuda_check("wt_step: shared-memory carve-out");
-        configured = true;
-    }
-    const auto& a = *static_cast<const StepArgs<typename P::S, typename P::T>*>(args);
-    const int32_t nchunks = (n + L - 1) / L;
-    const int32_t grid = std::min(nchunks, num_sms() * MINB);
-    k_step_stream<PREC, FAST, L, NS, THREADS, MINB, CPT><<<grid, THREADS, SMEM, st>>>(a);
-    return WT_OK;
-}
-
-#define WT_VARIANTS(PREC, FAST)                                                          \
-    {1, 0, 1, 256, 4, 0, 0, launch_bulk<PREC, FAST, 1, 256, 4>},                         \
-    {2, 0, 1, 128, 8, 0, 0, launch_bulk<PREC, FAST, 1, 128, 8>},                         \
-    {3, 0, 2, 128, 6, 0, 0, launch_bulk<PREC, FAST, 2, 128, 6>},                         \
-    {4, 0, 2, 128, 4, 0, 0, launch_bulk<PREC, FAST, 2, 128, 4>},                         \
-    {5, 0, 4, 128, 4, 0, 0, launch_bulk<PREC, FAST, 4, 128, 4>},                         \
-    {6, 0, 4, 128, 3, 0, 0, launch_bulk<PREC, FAST, 4, 128, 3>},                         \
-    {7, 0, 2, 256, 3, 0, 0, launch_bulk<PREC, FAST, 2, 256, 3>},                         \
-    {8, 1, 1, 512, 2, 480, 3, launch_stream<PREC, FAST, 480, 3, 512, 2, 1>},             \
-    {9, 1, 1, 512, 2, 480, 2, launch_stream<PREC, FAST, 480, 2, 512, 2, 1>},             \
-    {10, 1, 1, 1024, 1, 992, 2, launch_stream<PREC, FAST, 992, 2, 1024, 1, 1>},          \
-    {11, 1, 2, 512, 1, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 1, 2>},            \
-    {12, 1, 1, 512, 2, 480, 4, launch_stream<PREC, FAST, 480, 4, 512, 2, 1>},            \
-    {13, 1, 2, 512, 2, 960, 2, launch_stream<PREC, FAST, 960, 2, 512, 2, 2>},            \
-    {14, 1, 2, 512, 1, 960, 3, launch_stream<PREC, FAST, 960, 3, 512, 1, 2>},            \
-    {15, 1, 2, 512, 1, 960, 4, launch_stream<PREC, FAST, 960, 4, 512, 1, 2>},            \
-    {16, 1, 2, 256, 2, 448, 4, launch_stream<PREC, FAST, 448, 4, 256, 2, 2>},            \
-    {17, 1, 2, 384, 1, 704, 4, launch_stream<PREC, FAST, 704, 4, 384, 1, 2>},            \
-    {18, 0, 2, 128, 8, 0, 0, launch_bulk<PREC, FAST, 2, 128, 8>}
-
-template <int PREC, bool FAST>
-const StepVariant* variants(int* count) {
-    static const StepVariant table[] = {WT_VARIANTS(PREC, FAST)};
-    *count = (int)(sizeof(table) / sizeof(table[0]));
-    return table;
-}
-
-// defaults until the autotuner has measured the tunnel: two cells per thread at 64
-// registers (the fastest shape at 33.5M cells in fp32, fp16 and bf16); fp64 needs 128
-// registers to avoid spills, so it keeps two cells per thread at 128 registers
-template <int PREC>
-const StepVariant* pick_variant(const wt_grid* g) {
-    int count;
-    const StepVariant* t = g->collision == WT_COLLIDE_FAST ? variants<PREC, true>(&count) : variants<PREC, false>(&count);
-    const int want = g->tile > 0 ? g->tile : (PREC == WT_F64 ? 4 : 18);
-    for (int k = 0; k < count; ++k) {
-        if (t[k].id != want) continue;
-        if (g->nx % t[k].v != 0) return nullptr;
-        if (PREC == WT_F64 && t[k].v == 4) return nullptr;
-        if (t[k].kind == 1 && g->nx % 16 != 0) return nullptr;  // 16-byte copies of rows and code bytes
-        return &t[k];
-    }
-    return nullptr;
-}
-
-template <int PREC>
-int step_impl(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
-              cudaStream_t stream) {
-    using P = Prec<PREC>;
-    using T = typename P::T;
-    using S = typename P::S;
-    StepArgs<S, T> a;
-    a.solid = g->solid;
-    a.code = g->code;
-    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-    a.nxy = g->nx * g->ny;
-    a.n = a.nxy * g->nz;
-    a.dnx = FastDiv((uint32_t)g->nx);
-    a.dny = FastDiv((uint32_t)g->ny);
-    a.uin = (T)uin; a.tau = (T)tau;
-    const T sm = (T)smag;
-    a.csmag = (T)25.4558441 * sm * sm;  // same left-to-right product as server/lbm.py:152
-    const StepVariant* var = pick_variant<PREC>(g);
-    if (!var) return wt_set_error(WT_ERR_ARG, "wt_step: no kernel variant for tile %d (nx=%d)", g->tile, g->nx);
-    for (int b = 0; b < 2; ++b) {
-        const uintptr_t al = reinterpret_cast<uintptr_t>(g->f[b]);
-        if (al % 16 != 0) return wt_set_error(WT_ERR_ARG, "wt_step: population buffer %d not 16-byte aligned", b);
-    }
-    if (reinterpret_cast<uintptr_t>(g->code) % 16 != 0)
-        return wt_set_error(WT_ERR_ARG, "wt_step: code buffer not 16-byte aligned");
-    a.status = g->status;
-    a.test_skip_chunk = g->test_skip_chunk;
-    set_shift(a, P::shifted ? (double)g->shift_u : 0.0);
-    constexpr int VEC = 16 / (int)sizeof(S);
-    const int32_t nface = a.nxy + a.nx * (a.nz - 2);
-    const unsigned nb_face = (unsigned)((nface + 255) / 256);
-    for (int32_t s = 0; s < steps; ++s) {
-        const S* fin = static_cast<const S*>(g->f[cur]);
-        S* fout = static_cast<S*>(g->f[cur ^ 1]);
-        for (int i = 0; i < Q; ++i) {
-            const int64_t off = cx(i) + (int64_t)cy(i) * a.nx + (int64_t)cz(i) * a.nxy;
-            a.src[i] = fin + (int64_t)i * a.n - off;
-            a.dst[i] = fout + (int64_t)i * a.n;
-            const int32_t r = (int32_t)(((-off) % VEC + VEC) % VEC);  // n and chunk starts are multiples of VEC
-            a.chunk_r[i] = r;
-            a.chunk_src[i] = a.src[i] - r;
-        }
-        a.fin = fin;
-        a.mac_prev = static_cast<const T*>(g->mac[cur]);
-        a.mac_cur = static_cast<T*>(g->mac[cur ^ 1]);
-        a.mac_all = (flags & WT_STEP_MAC_ALL_LAST) && s == steps - 1;
-        if (int rc = var->launch(&a, a.n, stream)) return rc;
-        k_step_faces<PREC><<<nb_face, 256, 0, stream>>>(a);
-        cur ^= 1;
-    }
-    return wt_cuda_check("wt_step launch");
-}
-
-}  // namespace wt
+// Single-tunnel step entry points (wt_step, wt_step_tiles). The kernels and their tile-variant
+// tables are instantiated per storage precision in wt_kernels_<prec>.cu (see wt_kernels.cuh).
+#include "wt_variants.cuh"
 
 extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag,
                        int32_t flags, void* stream) {
@@ -155,10 +14,10 @@ extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin,
         return wt_set_error(WT_ERR_ARG, "wt_step: unknown collision form %d", g->collision);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch (g->precision) {
-        case WT_F32: return wt::step_impl<WT_F32>(g, cur, steps, uin, tau, smag, flags, st);
-        case WT_F16: return wt::step_impl<WT_F16>(g, cur, steps, uin, tau, smag, flags, st);
-        case WT_BF16: return wt::step_impl<WT_BF16>(g, cur, steps, uin, tau, smag, flags, st);
-        case WT_F64: return wt::step_impl<WT_F64>(g, cur, steps, uin, tau, smag, flags, st);
+        case WT_F32: return wt::step_prec<WT_F32>(g, cur, steps, uin, tau, smag, flags, st);
+        case WT_F16: return wt::step_prec<WT_F16>(g, cur, steps, uin, tau, smag, flags, st);
+        case WT_BF16: return wt::step_prec<WT_BF16>(g, cur, steps, uin, tau, smag, flags, st);
+        case WT_F64: return wt::step_prec<WT_F64>(g, cur, steps, uin, tau, smag, flags, st);
         default: return wt_set_error(WT_ERR_ARG, "wt_step: unknown precision %d", g->precision);
     }
 }
@@ -167,18 +26,18 @@ extern "C" int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap) {
     int count = 0;
     const wt::StepVariant* t = nullptr;
     switch (precision) {
-        case WT_F32: t = wt::variants<WT_F32, false>(&count); break;
-        case WT_F16: t = wt::variants<WT_F16, false>(&count); break;
-        case WT_BF16: t = wt::variants<WT_BF16, false>(&count); break;
-        case WT_F64: t = wt::variants<WT_F64, false>(&count); break;
+        case WT_F32: t = wt::step_variants<WT_F32>(false, &count); break;
+        case WT_F16: t = wt::step_variants<WT_F16>(false, &count); break;
+        case WT_BF16: t = wt::step_variants<WT_BF16>(false, &count); break;
+        case WT_F64: t = wt::step_variants<WT_F64>(false, &count); break;
         default: return wt_set_error(WT_ERR_ARG, "wt_step_tiles: unknown precision %d", precision);
     }
     for (int k = 0; k < count && k < cap; ++k) {
         if (!out) break;
         out[4 * k + 0] = t[k].id;
-        out[4 * k + 1] = t[k].kind == 0 ? t[k].v : -t[k].chunk;  // negative: streaming chunk length
+        out[4 * k + 1] = t[k].kind == 1 ? -t[k].chunk : t[k].v;  // negative: streaming chunk length
         out[4 * k + 2] = t[k].block;
-        out[4 * k + 3] = t[k].kind == 0 ? t[k].minb : t[k].stages;
+        out[4 * k + 3] = t[k].kind == 1 ? t[k].stages : t[k].minb;
     }
     return count;
 }
