@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define WT_ABI_VERSION 2
+#define WT_ABI_VERSION 3
 
 enum {
     WT_OK = 0,
@@ -71,8 +71,6 @@ typedef struct wt_grid {
     int32_t tile;          /* step kernel tile variant (wt_step_tiles); 0 = library default */
     int32_t collision;     /* WT_COLLIDE_EXACT (reference operation order) or WT_COLLIDE_FAST */
     int32_t* status;       /* optional device int: set to WT_ERR_TIMEOUT if a bounded wait gives up */
-    int32_t test_skip_chunk; /* test hook for the failure path: 0 = off; k > 0: chunk k-1 of a
-                                streaming tile is never loaded, so its bounded wait expires */
     float shift_u;         /* fp16/bf16 storage shift velocity U (see WT_F16); ignored otherwise.
                               Must equal the shift_u the buffers were initialised with. */
 } wt_grid;
@@ -119,6 +117,13 @@ int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap);
  * gives. Each step is two kernels. */
 int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
             void* stream);
+/* Test entry point for the failure path; no counterpart in the reference. wt_step with chunk
+ * skip_chunk - 1 (skip_chunk > 0) of a streaming tile never loaded, so the kernel's bounded
+ * wait for it runs out: the kernel sets *wt_grid.status to WT_ERR_TIMEOUT and returns, the
+ * context stays usable and the tunnel's populations are invalid until the next reset. Only
+ * streaming tiles (a negative second field in wt_step_tiles) wait; other tiles ignore it. */
+int wt_step_test_skip_chunk(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag,
+                            int32_t flags, int32_t skip_chunk, void* stream);
 
 /* Momentum-exchange force (force_kernel, server/lbm.py:169-197, run by Solver.frame
  * :479-481) on f[cur] over the compacted link list. out6 (device, 6 doubles):
@@ -135,7 +140,8 @@ int wt_forces(const wt_grid* g, int32_t cur, const int32_t* cells, const uint32_
  * allocation would synchronise the device). The block partials live in a 192 KB array
  * compiled into libwt.so, held by every GPU that loads the library until exit. At most
  * WT_NOALLOC_MAX_LINKS link cells per call (WT_ERR_CAPACITY beyond). The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress); make that first call
+ * device looks up the array's device address (cudaGetSymbolAddress), and so does the first
+ * call after that device's context was re-created (cudaDeviceReset); make such a call
  * before any stream capture. All calls share the array: calls whose kernels overlap on the
  * GPU race and must not be issued. Results equal wt_forces to fp64 rounding (the blocks
  * partition the list differently). */

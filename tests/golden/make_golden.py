@@ -7,9 +7,10 @@ text and the hand-written ``advect_kernel``/``pack_particles``/``slice_kernel``/
 float64) scalars. The outputs are written as small ``.npz`` fixtures beside this script;
 tests pin the C++ oracle and the CUDA kernels to them.
 
-Usage (needs the reference checkout; the fixtures themselves are committed):
-    python tests/golden/make_golden.py /root/reference            # solver fixtures
-    python tests/golden/make_golden.py /root/reference --frames   # wire frames (frames.npz)
+Usage (needs the reference checkout; the fixtures themselves are committed). The checkout's
+root is the first argument, or the environment variable WT_REFERENCE_ROOT:
+    python tests/golden/make_golden.py <reference root>            # solver fixtures
+    python tests/golden/make_golden.py <reference root> --frames   # wire frames (frames.npz)
 """
 import hashlib
 import json
@@ -213,8 +214,19 @@ def frames(ref):
     np.savez_compressed(os.path.join(HERE, 'frames.npz'), **out)
 
 
+def reference_root(argv):
+    """The reference checkout: the first non-option argument, else $WT_REFERENCE_ROOT."""
+    args = [a for a in argv[1:] if not a.startswith('--')]
+    ref = args[0] if args else os.environ.get('WT_REFERENCE_ROOT')
+    if not ref:
+        sys.exit('usage: make_golden.py <reference root> [--frames] (or set WT_REFERENCE_ROOT)')
+    if not os.path.exists(os.path.join(ref, 'server', 'lbm.py')):
+        sys.exit(f'{ref!r} does not hold server/lbm.py of the reference')
+    return ref
+
+
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    ref = reference_root(sys.argv)
     if '--frames' in sys.argv:
         frames(ref)
         return

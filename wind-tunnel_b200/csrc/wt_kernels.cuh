@@ -40,10 +40,32 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     return WT_OK;
 }
 
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR>
+static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
+    using P = Prec<PREC>;
+    using S = typename P::S;
+    using T = typename P::T;
+    (void)n;
+    RowArgs<S, T> r;
+    r.a = *static_cast<const StepArgs<S, T>*>(args);
+    const StepArgs<S, T>& a = r.a;
+    for (int i = 0; i < Q; ++i) {
+        // the pair of population i is pulled from cells idx - (cy, cz) (the x shift cancels
+        // against the pair's alignment)
+        r.loff[i] = ((int64_t)i * a.n - (int64_t)cy(i) * a.nx - (int64_t)cz(i) * a.nxy) * (int64_t)sizeof(S);
+        r.soff[i] = (int64_t)i * a.n * (int64_t)sizeof(S);
+    }
+    const dim3 grid((unsigned)((a.nx / 2 + BLOCK - 1) / BLOCK), (unsigned)a.ny, (unsigned)a.nz);
+    k_step_rows<PREC, FAST, BLOCK, MINB, ADDR><<<grid, BLOCK, 0, st>>>(r);
+    return WT_OK;
+}
+
 // Tile variants. Direct-load forms (kind 0): cells per thread (V), threads per block, minimum
 // resident blocks per SM. Streaming forms (kind 1): chunk length L, pipeline stages NS,
-// threads per block, blocks per SM. wt_grid.tile selects one (0 = the default for the
-// precision); autotune.py times them.
+// threads per block, blocks per SM. Row-grid forms (kind 2, k_step_rows): two cells per
+// thread, threads per block, minimum resident blocks per SM, and in the last field the
+// addressing form (0: per-population bases, 1: one base plus byte offsets). wt_grid.tile
+// selects one (0 = the default for the precision and collision form); autotune.py times them.
 #define WT_VARIANTS(PREC, FAST)                                                          \
     {1, 0, 1, 256, 4, 0, 0, launch_bulk<PREC, FAST, 1, 256, 4>},                         \
     {2, 0, 1, 128, 8, 0, 0, launch_bulk<PREC, FAST, 1, 128, 8>},                         \
@@ -62,7 +84,15 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     {15, 1, 2, 512, 1, 960, 4, launch_stream<PREC, FAST, 960, 4, 512, 1, 2>},            \
     {16, 1, 2, 256, 2, 448, 4, launch_stream<PREC, FAST, 448, 4, 256, 2, 2>},            \
     {17, 1, 2, 384, 1, 704, 4, launch_stream<PREC, FAST, 704, 4, 384, 1, 2>},            \
-    {18, 0, 2, 128, 8, 0, 0, launch_bulk<PREC, FAST, 2, 128, 8>}
+    {18, 0, 2, 128, 8, 0, 0, launch_bulk<PREC, FAST, 2, 128, 8>},                        \
+    {19, 2, 2, 128, 8, 0, 0, launch_rows<PREC, FAST, 128, 8, 0>},                        \
+    {20, 2, 2, 128, 8, 0, 1, launch_rows<PREC, FAST, 128, 8, 1>},                        \
+    {21, 2, 2, 64, 16, 0, 0, launch_rows<PREC, FAST, 64, 16, 0>},                        \
+    {22, 2, 2, 64, 16, 0, 1, launch_rows<PREC, FAST, 64, 16, 1>},                        \
+    {23, 2, 2, 256, 4, 0, 1, launch_rows<PREC, FAST, 256, 4, 1>},                        \
+    {24, 2, 2, 128, 4, 0, 0, launch_rows<PREC, FAST, 128, 4, 0>},                        \
+    {25, 2, 2, 128, 9, 0, 0, launch_rows<PREC, FAST, 128, 9, 0>},                        \
+    {26, 2, 2, 128, 10, 0, 0, launch_rows<PREC, FAST, 128, 10, 0>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants_of(int* count) {
@@ -96,7 +126,7 @@ const StepVariant* pick_variant(const wt_grid* g) {
 
 template <int PREC>
 int step_prec(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
-              cudaStream_t stream) {
+              int32_t skip_chunk, cudaStream_t stream) {
     using P = Prec<PREC>;
     using T = typename P::T;
     using S = typename P::S;
@@ -120,7 +150,7 @@ int step_prec(const wt_grid* g, int32_t cur, int32_t steps, double uin, double t
     if (reinterpret_cast<uintptr_t>(g->code) % 16 != 0)
         return wt_set_error(WT_ERR_ARG, "wt_step: code buffer not 16-byte aligned");
     a.status = g->status;
-    a.test_skip_chunk = g->test_skip_chunk;
+    a.test_skip_chunk = skip_chunk;
     set_shift(a, P::shifted ? (double)g->shift_u : 0.0);
     constexpr int VEC = 16 / (int)sizeof(S);
     const int32_t nface = a.nxy + a.nx * (a.nz - 2);
@@ -229,6 +259,6 @@ const BatchVariant* batch_variant(bool fast, int id) {
 #define WT_INSTANTIATE(PREC)                                                                                       \
     namespace wt {                                                                                                 \
     template const StepVariant* step_variants<PREC>(bool, int*);                                                   \
-    template int step_prec<PREC>(const wt_grid*, int32_t, int32_t, double, double, double, int32_t, cudaStream_t); \
+    template int step_prec<PREC>(const wt_grid*, int32_t, int32_t, double, double, double, int32_t, int32_t, cudaStream_t); \
     template const BatchVariant* batch_variant<PREC>(bool, int);                                                   \
     }

@@ -218,23 +218,59 @@ extern "C" int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* 
 constexpr int NOALLOC_MAX_BLOCKS = 4096;
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_BLOCKS * FORCE_VALS];
 
-// Device address of g_noalloc_partials for the current device, looked up once per device
-// (the host-side symbol is only a stand-in and must never be passed to a kernel).
+// The current thread's CUDA context as a process-unique id (driver cuCtxGetCurrent +
+// cuCtxGetId, fetched through the runtime so the library needs no link to libcuda); 0 when
+// no context is current or the driver lacks the entry points.
+static unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+                       q == cudaDriverEntryPointSuccess
+                   ? reinterpret_cast<GetCurrent>(fn)
+                   : nullptr;
+    }();
+    static GetId get_id = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+                       q == cudaDriverEntryPointSuccess
+                   ? reinterpret_cast<GetId>(fn)
+                   : nullptr;
+    }();
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of g_noalloc_partials in the current device's context, looked up on the
+// first call on each device and again whenever that device's context has been re-created
+// (after cudaDeviceReset, say): the host-side symbol is only a stand-in and must never be
+// passed to a kernel, and an address from a destroyed context must not be reused.
 static int noalloc_scratch(double** out) {
+    struct Entry {
+        unsigned long long ctx;
+        double* addr;
+    };
     static std::mutex mu;
-    static double* addr[128] = {};
+    static Entry cache[128] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
         return wt_set_error(WT_ERR_CUDA, "wt_forces_noalloc: no current CUDA device");
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!cache[dev].addr || ctx == 0 || cache[dev].ctx != ctx) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);  // makes the context current
         if (e != cudaSuccess || !p)
             return wt_set_error(WT_ERR_CUDA, "wt_forces_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        addr[dev] = static_cast<double*>(p);
+        cache[dev].addr = static_cast<double*>(p);
+        cache[dev].ctx = current_context_id();
     }
-    *out = addr[dev];
+    *out = cache[dev].addr;
     return WT_OK;
 }
 

@@ -2,8 +2,8 @@
 // tables are instantiated per storage precision in wt_kernels_<prec>.cu (see wt_kernels.cuh).
 #include "wt_variants.cuh"
 
-extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag,
-                       int32_t flags, void* stream) {
+static int step_any(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag,
+                    int32_t flags, int32_t skip_chunk, void* stream) {
     if (!g || !g->f[0] || !g->f[1] || !g->mac[0] || !g->mac[1] || !g->solid || !g->code)
         return wt_set_error(WT_ERR_ARG, "wt_step: null buffer in grid");
     if (int rc = wt_check_dims(g->nx, g->ny, g->nz)) return rc;
@@ -14,12 +14,23 @@ extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin,
         return wt_set_error(WT_ERR_ARG, "wt_step: unknown collision form %d", g->collision);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch (g->precision) {
-        case WT_F32: return wt::step_prec<WT_F32>(g, cur, steps, uin, tau, smag, flags, st);
-        case WT_F16: return wt::step_prec<WT_F16>(g, cur, steps, uin, tau, smag, flags, st);
-        case WT_BF16: return wt::step_prec<WT_BF16>(g, cur, steps, uin, tau, smag, flags, st);
-        case WT_F64: return wt::step_prec<WT_F64>(g, cur, steps, uin, tau, smag, flags, st);
+        case WT_F32: return wt::step_prec<WT_F32>(g, cur, steps, uin, tau, smag, flags, skip_chunk, st);
+        case WT_F16: return wt::step_prec<WT_F16>(g, cur, steps, uin, tau, smag, flags, skip_chunk, st);
+        case WT_BF16: return wt::step_prec<WT_BF16>(g, cur, steps, uin, tau, smag, flags, skip_chunk, st);
+        case WT_F64: return wt::step_prec<WT_F64>(g, cur, steps, uin, tau, smag, flags, skip_chunk, st);
         default: return wt_set_error(WT_ERR_ARG, "wt_step: unknown precision %d", g->precision);
     }
+}
+
+extern "C" int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag,
+                       int32_t flags, void* stream) {
+    return step_any(g, cur, steps, uin, tau, smag, flags, 0, stream);
+}
+
+extern "C" int wt_step_test_skip_chunk(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau,
+                                       double smag, int32_t flags, int32_t skip_chunk, void* stream) {
+    if (skip_chunk < 0) return wt_set_error(WT_ERR_ARG, "wt_step_test_skip_chunk: skip_chunk < 0");
+    return step_any(g, cur, steps, uin, tau, smag, flags, skip_chunk, stream);
 }
 
 extern "C" int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap) {

@@ -350,9 +350,29 @@ struct F2 {
     __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
 };
 __device__ __forceinline__ F2 operator+(F2 a, F2 b) { F2 r; r.v = __fadd2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { F2 r; r.v = __fmul2_rn(a.v, b.v); return r; }
+#ifndef WT_PAIRED_SUB
+#define WT_PAIRED_SUB 0
+#endif
+#if WT_PAIRED_SUB == 0
 __device__ __forceinline__ F2 operator-(F2 a) { return F2(-a.v.x, -a.v.y); }
 __device__ __forceinline__ F2 operator-(F2 a, F2 b) { return a + (-b); }  // x - y == x + (-y) in IEEE
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) { F2 r; r.v = __fmul2_rn(a.v, b.v); return r; }
+#else
+__device__ __forceinline__ F2 operator-(F2 a) { return a * F2(-1.0); }  // exact negation, one paired op
+#if WT_PAIRED_SUB == 1
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {  // paired IEEE subtraction
+    unsigned long long x, y, d;
+    memcpy(&x, &a.v, 8);
+    memcpy(&y, &b.v, 8);
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(x), "l"(y));
+    F2 r;
+    memcpy(&r.v, &d, 8);
+    return r;
+}
+#else
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return a + b * F2(-1.0); }
+#endif
+#endif
 __device__ __forceinline__ F2 fmaT(F2 a, F2 b, F2 c) { F2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r; }
 __device__ __forceinline__ F2 rcp_fast(F2 x) {
     float r0, r1;
@@ -811,6 +831,34 @@ __device__ __forceinline__ void pair_unpack(const A& a, const PairRaw<typename P
 // populations are not written. The results and mac writes are those of general_cell and
 // outlet_cell, but a warp no longer splits into per-cell branches at walls and row ends.
 // pair_finish takes the pulled populations; interior_pair loads them itself.
+// Bounce-back and moving belt (server/lbm.py:110-124) as overrides of a pair's pulled values:
+// for each cell of the pair next to a non-fluid cell (CODE_NEAR in c0 / c1), every population
+// whose source is non-fluid takes the cell's own opposite population instead.
+template <int PREC, bool FAST>
+__device__ __forceinline__ void pair_walls(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                           int32_t idx0, uint32_t c0, uint32_t c1, typename Prec<PREC>::T (&f)[2][Q]) {
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    unroll<1, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const int32_t off = cx(i) + cy(i) * a.nx + cz(i) * a.nxy;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (((k ? c1 : c0) & CODE_NEAR) == 0) continue;
+            const int t = a.solid[idx0 + k - off];
+            if (t != 0) {
+                // bounce-back; in deviation form the shift difference e_opp(i) - e_i is added
+                T b = ld_in<P, FAST, opp(i)>(a, a.fin + (int64_t)opp(i) * a.n + idx0 + k);
+                if constexpr (FAST && P::shifted) b = b + a.bb[i];
+                if constexpr (cx(i) != 0) {
+                    if (t == 2) b = b + (T)(6.0 * wd(i) * cx(i)) * a.uin;
+                }
+                f[k][i] = b;
+            }
+        }
+    });
+}
+
 template <int PREC, bool FAST>
 __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                             int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
@@ -828,26 +876,7 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
         if (wsol1) store_mac(a.mac_cur, idx0 + 1, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
         return;
     }
-    if ((c0 | c1) & CODE_NEAR) {
-        unroll<1, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            const int32_t off = cx(i) + cy(i) * a.nx + cz(i) * a.nxy;
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                if (((k ? c1 : c0) & CODE_NEAR) == 0) continue;
-                const int t = a.solid[idx0 + k - off];
-                if (t != 0) {
-                    // bounce-back; in deviation form the shift difference e_opp(i) - e_i is added
-                    T b = ld_in<P, FAST, opp(i)>(a, a.fin + (int64_t)opp(i) * a.n + idx0 + k);
-                    if constexpr (FAST && P::shifted) b = b + a.bb[i];
-                    if constexpr (cx(i) != 0) {
-                        if (t == 2) b = b + (T)(6.0 * wd(i) * cx(i)) * a.uin;
-                    }
-                    f[k][i] = b;
-                }
-            }
-        });
-    }
+    if ((c0 | c1) & CODE_NEAR) pair_walls<PREC, FAST>(a, idx0, c0, c1, f);
     T m[2][4];
     collide_two<P, FAST>(a, f, x0, m);
     if (sol0) {  // a solid cell's macro values are (0, 0, 0, 1); the outlet may read them
@@ -1034,6 +1063,106 @@ __global__ void __launch_bounds__(256) k_step_faces(const StepArgs<typename Prec
 }
 
 // ---------------------------------------------------------------------------------
+// Row-grid form of the two-cell tile. The grid is (x-runs, ny, nz): a block covers 2 * BLOCK
+// consecutive cells of one lattice row, so the row's y and z come from the block index (no
+// division) and the face-row and shell-row tests are uniform over the block. A warp of an
+// interior row whose 64 cells are all fluid takes a lean path: pull, pair collision and stores,
+// with the few lanes next to a wall, at the inlet or at the outlet applying their boundary
+// rule as a per-lane override (pair_walls, eq_values), as pair_finish does. A warp holding a
+// solid cell runs interior_pair, and face rows run bulk_cells, so the results are bit for bit
+// those of the one-dimensional two-cell tiles.
+//
+// Addressing (ADDR): 0 -- population i is pulled from src[i] + idx0 and stored to
+// dst[i] + idx0, one wide multiply-add of a kernel-parameter base per population; 1 -- from one
+// per-thread base fin + idx0 plus a per-population byte offset computed on the host
+// (RowArgs::loff, soff), one 64-bit add per population.
+// ---------------------------------------------------------------------------------
+template <class S, class T>
+struct RowArgs {
+    StepArgs<S, T> a;
+    int64_t loff[Q];  // bytes from fin + idx0 to the aligned pull pair of population i
+    int64_t soff[Q];  // bytes from fout + idx0 to population i of the output
+};
+
+template <int PREC, bool FAST, int ADDR>
+__device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
+                                          int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
+                                          bool row_shell) {
+    using P = Prec<PREC>;
+    using S = typename P::S;
+    using T = typename P::T;
+    const auto& a = r.a;
+    const int32_t nx = a.nx;
+    const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * (int64_t)sizeof(S);
+    T f[2][Q];
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        // the aligned pair holding the pull sources of both cells but for the x-shifted one; the
+        // shifted one lies just outside it, inside the row: x0 - 1 >= 0 when cx > 0 pulls into
+        // x0 > 0, and the inlet cell x0 = 0 has a source at x = -1 only in its own (discarded)
+        // pull, which reads the previous row's last cell, still inside the buffer
+        const S* p = ADDR == 0 ? a.src[i] + idx0 + cx(i) : reinterpret_cast<const S*>(fb + r.loff[i]);
+        const SVec<S, 2> v = vload<S, 2>(p);
+        if constexpr (cx(i) == 0) {
+            f[0][i] = ld_in<P, FAST, i>(a, &v.v[0]);
+            f[1][i] = ld_in<P, FAST, i>(a, &v.v[1]);
+        } else if constexpr (cx(i) > 0) {
+            f[0][i] = ld_in<P, FAST, i>(a, p - 1);
+            f[1][i] = ld_in<P, FAST, i>(a, &v.v[0]);
+        } else {
+            f[0][i] = ld_in<P, FAST, i>(a, &v.v[1]);
+            f[1][i] = ld_in<P, FAST, i>(a, p + 2);
+        }
+    });
+    const uint32_t c0 = codes & 0xffu, c1 = codes >> 8;
+    if ((c0 | c1) & CODE_NEAR) pair_walls<PREC, FAST>(a, idx0, c0, c1, f);  // lanes next to a wall
+    T m[2][4];
+    collide_two<P, FAST>(a, f, x0, m);
+    const bool inlet = x0 == 0, outlet = x0 + 2 == nx;
+    if (inlet) {  // x = 0: the inlet equilibrium replaces the collision (server/lbm.py:96-99)
+        eq_values<P, FAST>(a, (T)1.0, a.uin, (T)0.0, (T)0.0, f[0]);
+        m[0][0] = a.uin; m[0][1] = (T)0.0; m[0][2] = (T)0.0; m[0][3] = (T)1.0;
+    } else if (outlet) {  // x = nx-1: the outlet from its x = nx-2 neighbour (server/lbm.py:100-103)
+        T br, bux, buy, buz;
+        face_values<T>(nx - 1, y, z, nx, a.ny, a.nz, a.uin, m[0][0], m[0][1], m[0][2], m[0][3], br, bux, buy, buz);
+        eq_values<P, FAST>(a, br, bux, buy, buz, f[1]);
+        m[1][0] = bux; m[1][1] = buy; m[1][2] = buz; m[1][3] = br;
+    }
+    char* ob = reinterpret_cast<char*>(a.dst[0]) + (int64_t)idx0 * (int64_t)sizeof(S);
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        store_cells<P, FAST, 2, i>(a, ADDR == 0 ? a.dst[i] + idx0 : reinterpret_cast<S*>(ob + r.soff[i]), f);
+    });
+    // mac where faces read it (coordinates 1 and n-2), and everywhere when mac_all
+    const bool w0 = a.mac_all || (!inlet && (row_shell || x0 == nx - 2));
+    const bool w1 = a.mac_all || (!outlet && (row_shell || inlet));
+    if (w0) store_mac(a.mac_cur, idx0, m[0][0], m[0][1], m[0][2], m[0][3]);
+    if (w1) store_mac(a.mac_cur, idx0 + 1, m[1][0], m[1][1], m[1][2], m[1][3]);
+}
+
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
+    const auto& a = r.a;
+    const int32_t y = (int32_t)blockIdx.y, z = (int32_t)blockIdx.z;
+    const int32_t nx = a.nx;
+    const int32_t x0 = ((int32_t)blockIdx.x * BLOCK + (int32_t)threadIdx.x) * 2;
+    const bool valid = x0 < nx;
+    const int32_t idx0 = x0 + nx * (y + a.ny * z);
+    if (y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1) {  // a face row (uniform over the block)
+        bulk_cells<PREC, FAST, 2>(a, idx0, valid);
+        return;
+    }
+    const bool row_shell = y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2;
+    const uint32_t codes = valid ? *reinterpret_cast<const uint16_t*>(a.code + idx0) : 0xffffu;
+    // lean unless a cell of the warp is solid (or past the row's end)
+    if (__all_sync(0xffffffffu, (codes & (CODE_SOLID * 0x0101u)) == 0)) {
+        pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell);
+    } else if (valid) {
+        interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell);
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Streaming form of the bulk kernel: shared-memory staging through bulk async copies.
 //
 // With pull streaming, the destination cells [c0, c0 + L) read population i from the
@@ -1077,11 +1206,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after WAIT_LIMIT tries, about a second.
-constexpr uint32_t WAIT_LIMIT = 1u << 20;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded waits. The suspend hint of try_wait is only an upper bound (a try may return early),
+// so the limit is time on the GPU's global nanosecond timer: a wait gives up WAIT_NS after its
+// first unsuccessful try. WAIT_TRIES also caps the tries (about a second at 30 ns a try), so a
+// wait ends even if the timer were to stand still. DRAIN_NS is the longer limit for copies
+// that were already issued and are only being waited out before the CTA exits.
+constexpr uint64_t WAIT_NS = 1000000000ull;
+constexpr uint64_t DRAIN_NS = 10000000000ull;
+constexpr uint32_t WAIT_TRIES = 1u << 25;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = WAIT_NS) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    const uint32_t tries = limit_ns > WAIT_NS ? WAIT_TRIES * (uint32_t)(limit_ns / WAIT_NS > 16 ? 16 : limit_ns / WAIT_NS)
+                                              : WAIT_TRIES;
+    for (uint32_t it = 0; it < tries; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
     return false;
 }
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -1228,11 +1374,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_stream(const StepArgs<ty
             }
             if (!stream_issue<PREC, L>(a, smem + (size_t)st * LY::STAGE_BYTES, &full[st], k)) continue;
         }
-        // keep the CTA's shared memory alive until every issued copy has landed (bounded)
+        // Keep the CTA's shared memory alive until every issued copy has landed. Issued copies
+        // always complete, so this waits DRAIN_NS (ten times the pipeline's limit) before it
+        // gives up; if it ever does, the tunnel is marked failed, because a copy could then
+        // still land in shared memory the CTA no longer owns.
         for (int32_t q = issued_lo; q < j; ++q) {
             const int32_t k = blockIdx.x + q * gridDim.x;
             if (k + 1 == a.test_skip_chunk) continue;
-            mbar_wait(&full[q % NS], (uint32_t)((q / NS) & 1));
+            if (!mbar_wait(&full[q % NS], (uint32_t)((q / NS) & 1), DRAIN_NS) && a.status)
+                atomicExch(a.status, WT_ERR_TIMEOUT);
         }
         return;
     }

@@ -41,10 +41,11 @@ struct BatchArgs {
 // the step variants of precision PREC for one collision form (fast = WT_COLLIDE_FAST)
 template <int PREC>
 const StepVariant* step_variants(bool fast, int* count);
-// `steps` steps of one tunnel (wt_step after argument checks)
+// `steps` steps of one tunnel (wt_step after argument checks; skip_chunk is the failure-path
+// test hook of wt_step_test_skip_chunk, 0 = off)
 template <int PREC>
 int step_prec(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
-              cudaStream_t stream);
+              int32_t skip_chunk, cudaStream_t stream);
 // the batched kernels of tile id `id`, or null
 template <int PREC>
 const BatchVariant* batch_variant(bool fast, int id);

@@ -55,6 +55,7 @@ import wire
 from batch import MemberError
 
 PAUSED_HZ = 12  # frames per second of a paused session (server/app.py:20)
+_SUBMIT = {'type': '_submit'}  # marks a session queued by enqueue() in the command deque
 
 
 class Session:
@@ -88,6 +89,7 @@ class Session:
         self.frame_no = 0
         self.ready = True          # client pacing: the client holds no unacknowledged frame
         self.verts = self.norms = None  # surface points for Cp, once uploaded
+        self.applied = []          # (frames before it, message, payload) per command, with keep_frames
 
     @property
     def running(self):
@@ -188,7 +190,9 @@ class SessionServer:
         waiting for memory keeps its parameters and uploads for when it is admitted. A
         resolution change ('grid') is a new session: its footprint goes through admission.
         command() and disconnect() may be called from other threads (a WebSocket front end's
-        handlers) while the serving thread runs rounds."""
+        handlers) while the serving thread runs rounds; a session queued from such a thread
+        goes through enqueue(), so that its commands cannot overtake it. A command for a
+        session that is not (or no longer) here is reported in ``errors``."""
         if msg.get('type') == 'grid':
             raise ValueError("a resolution change is a new session; submit one")
         self._cmds.append((sid, dict(msg), payload))
@@ -214,14 +218,23 @@ class SessionServer:
     def _apply_commands(self, now):
         for _ in range(len(self._cmds)):  # those queued before this round; later ones wait
             sid, msg, payload = self._cmds.popleft()
+            if msg is _SUBMIT:
+                self.submit(payload)
+                continue
             s = self.active.get(sid)
             if s is None:
                 s = next((q for q in self.queue if q.id == sid), None)
             if s is None:
-                continue  # gone, or never here: the reference ignores commands without a solver
+                # gone (retired, failed, disconnected) or never here: the reference ignores
+                # commands without a solver; a command, unlike a late disconnect, is reported
+                if msg is not None:
+                    self.errors.append((sid, f"command {msg.get('type')!r} for no session"))
+                continue
             if msg is None:  # disconnected: the lifetime ends now (retired or abandoned below)
                 s.lifetime = min(s.lifetime, now - s.arrival)
                 continue
+            if self.keep_frames:  # which frames each command came before (test replays)
+                s.applied.append((s.frame_no, dict(msg), payload))
             try:
                 self._apply(s, msg, payload, now)
             except Exception as e:  # a bad message fails alone (the Engine reports it, server/app.py:160-161)
@@ -238,14 +251,17 @@ class SessionServer:
             old = int(s.p.get('particles', s.particles))
             s.p.update({k: v for k, v in msg.items() if k != 'type'})
             new = int(s.p.get('particles', old))
-            if new != old:
+            # a new count re-seeds only a tunnel that has particles (server/app.py:128-131)
+            if new != old and (sv.num_p if sv is not None else s.particles):
                 s.particles = new
-                if sv is not None and sv.num_p:
+                if sv is not None:
                     sv.set_particles(new, s.p)
             self._invalidate(s)
         elif t == 'respawn':
             if sv is not None:
                 sv.set_particles(int(s.p.get('particles', s.particles)), s.p)
+            else:  # still waiting for memory: the tunnel gets its particles when it is created
+                s.particles = int(s.p.get('particles', s.particles))
         elif t == 'reset':
             if sv is not None:
                 self._invalidate(s)
@@ -256,6 +272,7 @@ class SessionServer:
                 return
             if got[0] == 'solid':
                 s.solid = got[1].copy()
+                s.frontal = bodies.areas(s.solid, s.dims)[0]
                 if sv is not None:
                     self._invalidate(s)
                     sv.set_solid(s.solid)
@@ -286,8 +303,16 @@ class SessionServer:
 
     # ---- admission ----
     def submit(self, session):
+        """Queue a session for admission now (the serving thread, or a single-threaded
+        driver)."""
         self.queue.append(session)
         self.max_queued = max(self.max_queued, len(self.queue))
+
+    def enqueue(self, session):
+        """Queue a session from another thread (a front end's handler): it joins the admission
+        queue when the next round starts, in order with the commands queued after it, so a
+        command sent right after enqueue() finds its session."""
+        self._cmds.append((session.id, _SUBMIT, session))
 
     def _admit(self, now):
         while self.queue:

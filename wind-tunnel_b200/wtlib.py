@@ -21,6 +21,7 @@ COLLIDE_EXACT, COLLIDE_FAST = 0, 1
 # every symbol include/wt.h declares (tests check that the library exports them all)
 EXPORTS = ['wt_last_error', 'wt_abi_version', 'wt_check_dims', 'wt_population_bytes', 'wt_init_eq',
            'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step_tiles', 'wt_step',
+           'wt_step_test_skip_chunk',
            'wt_reduce_scratch_len', 'wt_forces', 'wt_forces_noalloc', 'wt_mass', 'wt_batch_workspace_bytes',
            'wt_batch_create', 'wt_batch_step', 'wt_batch_capture', 'wt_batch_replay', 'wt_batch_cur',
            'wt_batch_destroy', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp',
@@ -40,11 +41,11 @@ class Grid(ctypes.Structure):
                 ('f', ctypes.c_void_p * 2), ('mac', ctypes.c_void_p * 2),
                 ('solid', ctypes.c_void_p), ('code', ctypes.c_void_p),
                 ('tile', ctypes.c_int32), ('collision', ctypes.c_int32),
-                ('status', ctypes.c_void_p), ('test_skip_chunk', ctypes.c_int32), ('shift_u', ctypes.c_float)]
+                ('status', ctypes.c_void_p), ('shift_u', ctypes.c_float)]
 
 
 _lib = None
-ABI_VERSION = 2  # include/wt.h WT_ABI_VERSION this binding is written against
+ABI_VERSION = 3  # include/wt.h WT_ABI_VERSION this binding is written against
 
 
 def lib():
@@ -68,6 +69,7 @@ def lib():
             'wt_links_fill': ([gp, vp, vp, vp, i64, vp], ctypes.c_int),
             'wt_step_tiles': ([i32, vp, i32], ctypes.c_int),
             'wt_step': ([gp, i32, i32, f64, f64, f64, i32, vp], ctypes.c_int),
+            'wt_step_test_skip_chunk': ([gp, i32, i32, f64, f64, f64, i32, i32, vp], ctypes.c_int),
             'wt_reduce_scratch_len': ([i64], i64),
             'wt_forces': ([gp, i32, vp, vp, i64, vp, vp, vp], ctypes.c_int),
             'wt_forces_noalloc': ([gp, i32, vp, vp, i64, vp, vp], ctypes.c_int),
