@@ -21,7 +21,7 @@ The line also carries, for the fp32 default run: `roofline` (the fused step alon
 HBM peak, with a 2 GiB device copy timed in the same run beside it), `cpu_baseline` (the
 oracle on the host cores), `precision_variants` (fp32 fast, fp16 and bf16 shifted storage,
 fp16 exact), `accuracy_vs_fp64` (a chaotic and a laminar regime against an fp64 run),
-`batching` (the 24-tunnel batch of config 4 under both batch executors, one tunnel re-run
+`batching` (the 24-tunnel batch of config 4 under both batch executors, every tunnel re-run
 alone and compared bit for bit), and `voxelize` (the server-side voxeliser on the benchmark
 body). At N = 1 it carries `serving`: the config-5 serving loop (Poisson sessions of
 0.5-33.5M cells under a 160 GB budget, 30 frames/s requested per session) run from its
@@ -96,7 +96,7 @@ def profile_traffic(name):
 
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
-    FIELDS = ['clocks.sm', 'clocks.max.sm', 'power.draw', 'clocks_event_reasons.hw_slowdown',
+    FIELDS = ['clocks.sm', 'clocks.max.sm', 'power.draw', 'utilization.gpu', 'clocks_event_reasons.hw_slowdown',
               'clocks_event_reasons.hw_thermal_slowdown', 'clocks_event_reasons.sw_thermal_slowdown',
               'clocks_event_reasons.sw_power_cap']
 
@@ -131,7 +131,9 @@ class ClockSampler:
             self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        """Median SM clock over the samples taken under load (GPU utilization >= 50%), the
+        maximum clock and every throttle reason seen active in any sample."""
+        sm, loaded, mx, reasons = [], [], None, set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(',')]
@@ -140,14 +142,17 @@ class ClockSampler:
             try:
                 sm.append(float(parts[0]))
                 mx = float(parts[1])
+                if float(parts[3]) >= 50.0:
+                    loaded.append(sm[-1])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[3:]):
+            for nm, v in zip(names, parts[4:]):
                 if v.lower().startswith('active'):
                     reasons.add(nm)
         if not sm:
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
-        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+        return {'sm_mhz': statistics.median(loaded or sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons),
+                'samples': len(sm), 'samples_under_load': len(loaded)}
 
 
 def frame_params(dims):
@@ -163,6 +168,24 @@ def build_workload(scale):
     dims, solid, p = bodies.config2(scale=scale)
     verts, norms = bodies.surface_points(solid, dims)
     return dims, solid, verts, norms
+
+
+STEP_REPEATS, STEP_CHUNK = 5, 50
+
+
+def step_time(solver, p, ev0, ev1):
+    """Seconds per LBM step: median of STEP_REPEATS timings of STEP_CHUNK steps each, CUDA
+    events on the tunnel's stream (the populations, 2.5-5 GB at 33.5M cells, exceed L2)."""
+    import torch
+    reps = []
+    for _ in range(STEP_REPEATS):
+        torch.cuda.synchronize(solver.dev)
+        ev0.record(solver.stream)
+        solver.step(STEP_CHUNK, p)
+        ev1.record(solver.stream)
+        ev1.synchronize()
+        reps.append(ev0.elapsed_time(ev1) / 1e3 / STEP_CHUNK)
+    return statistics.median(reps), reps
 
 
 def run_ours(args, rank, world, local_rank):
@@ -206,25 +229,20 @@ def run_ours(args, rank, world, local_rank):
     s.synchronize()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        torch.cuda.synchronize(dev)
-        ev0.record(s.stream)
-        for _ in range(args.steps):
-            frame_device()
-        ev1.record(s.stream)
-        torch.cuda.synchronize(dev)
+    # the clock sampler runs across every device-timed region below (frames, step, variants)
+    clk = ClockSampler(local_rank).__enter__()
+    torch.cuda.synchronize(dev)
+    ev0.record(s.stream)
+    for _ in range(args.steps):
+        frame_device()
+    ev1.record(s.stream)
+    torch.cuda.synchronize(dev)
     barrier()
     t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     value = ranks.whole_job_rate(n * STEPS_PER_FRAME * args.steps, t_dev) / 1e9
 
     # ---- LBM step alone: roofline of the fused step (bulk + face kernels) ----
-    nstep = max(20, args.steps)
-    torch.cuda.synchronize(dev)
-    ev0.record(s.stream)
-    s.step(nstep, p)
-    ev1.record(s.stream)
-    torch.cuda.synchronize(dev)
-    t_step = ev0.elapsed_time(ev1) / 1e3 / nstep
+    t_step, step_reps = step_time(s, p, ev0, ev1)
     hbm, peak_kind = peaks()
     achieved = ALGO_BYTES[prec] * n / t_step / 1e9
     copy_here = copy_bandwidth(dev)
@@ -236,6 +254,8 @@ def run_ours(args, rank, world, local_rank):
                 'algorithmic_bytes_per_cell': ALGO_BYTES[prec], 'step_ms': round(t_step * 1e3, 4),
                 'copy_gbs_this_run': round(copy_here, 1), 'frac_of_copy_this_run': round(achieved / copy_here, 4),
                 'glups_step_only': round(n / t_step / 1e9, 3), 'tile': tile,
+                'timing': f'median of {STEP_REPEATS} repeats of {STEP_CHUNK} steps (CUDA events on the tunnel stream)',
+                'step_ms_repeats': [round(x * 1e3, 4) for x in step_reps],
                 'tile_ms_per_step': {str(k): round(v, 4) for k, v in tile_ms.items()}}
     del s
     torch.cuda.empty_cache()
@@ -282,18 +302,15 @@ def run_ours(args, rank, world, local_rank):
             v.reset(p['uIn'])
             vtile, vms = autotune.tune(v, p, force=True)
             v.step(5, p)
-            torch.cuda.synchronize(dev)
-            ev0.record(v.stream)
-            v.step(nstep, p)
-            ev1.record(v.stream)
-            torch.cuda.synchronize(dev)
-            tv = ev0.elapsed_time(ev1) / 1e3 / nstep
+            tv, _ = step_time(v, p, ev0, ev1)
             variants[f'{vp}-{vc}'] = {'glups_step_only': round(n / tv / 1e9, 3),
                             'achieved_gbs': round(ALGO_BYTES[vp] * n / tv / 1e9, 1),
                             'speedup_vs_fp32_step': round(t_step / tv, 3), 'tile': vtile,
                             'tile_ms_per_step': {str(k): round(x, 4) for k, x in vms.items()}}
             del v
             torch.cuda.empty_cache()
+
+    clk.__exit__(None, None, None)
 
     batching = run_batching(dev) if args.batch and prec == 'fp32' else None
     vox = run_voxelize(dev) if args.batch and prec == 'fp32' else None
@@ -314,8 +331,9 @@ def run_batching(dev, replays=5, graph_steps=100):
     batch: persistent bulk kernel over a tile work-list plus a face kernel per step, captured
     as a CUDA graph of `graph_steps` steps. The batch tile is picked by timing each batched
     tile shape. The streams executor (every tunnel's own kernel on its own stream, forked and
-    joined inside one graph) is timed the same way. One tunnel is then re-run alone, for
-    every step both executors made, and compared bit for bit."""
+    joined inside one graph) is timed the same way. Every tunnel is then re-run alone for
+    every step both executors made and compared bit for bit (populations, mac, forces), with
+    its rate alone beside it."""
     import torch
     import bodies
     import lbm
@@ -331,7 +349,7 @@ def run_batching(dev, replays=5, graph_steps=100):
     cells = sum(s.n for s in solvers)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tile_ms, steps_done = {}, 0
-    for tile in (1, 2, 3, 7, 18):
+    for tile in (3, 7, 18, 103, 104, 118):  # persistent forms, then the grid forms (100 + k)
         b = TunnelBatch(solvers, params, tile=tile)
         b.step(2)
         ev0.record(b.stream)
@@ -370,21 +388,38 @@ def run_batching(dev, replays=5, graph_steps=100):
     steps_done += replays * graph_steps
     ts = ev0.elapsed_time(ev1) / 1e3
     b.close()
-    k = min(range(len(solvers)), key=lambda i: solvers[i].n)
-    dims, solid, p = cfg[k]
-    alone = lbm.Solver(dims, dev)
-    alone.set_solid(solid)
-    alone.reset(p['uIn'])
-    alone.step(steps_done, p)
-    same = bool(np.array_equal(alone.populations(), solvers[k].populations()))
+    # every tunnel re-run alone for the same steps: populations compared bit for bit on the
+    # device, forces (fp64, deterministic) exactly, and the tunnel's own rate alone
+    per, alone_s = [], 0.0
+    for k, (dims, solid, p) in enumerate(cfg):
+        alone = lbm.Solver(dims, dev)
+        alone.set_solid(solid)
+        alone.reset(p['uIn'])
+        ev0.record(alone.stream)
+        alone.step(steps_done, p)
+        ev1.record(alone.stream)
+        ev1.synchronize()
+        ta = ev0.elapsed_time(ev1) / 1e3
+        alone_s += ta
+        b_s = solvers[k]
+        same = bool(torch.equal(alone.f[alone.cur], b_s.f[b_s.cur]) and torch.equal(alone.mac[alone.cur], b_s.mac[b_s.cur]))
+        f_alone, f_batch = alone.forces6(), b_s.forces6()
+        per.append({'dims': list(dims), 'cells': alone.n, 'bit_identical': same,
+                    'forces_identical': bool(np.array_equal(f_alone, f_batch)),
+                    'cd_batch': round(float(f_batch[3] / (0.5 * p['uIn'] ** 2 * max(1, bodies.areas(solid, dims)[0]))), 6),
+                    'alone_glups': round(alone.n * steps_done / ta / 1e9, 3)})
+        del alone
+    torch.cuda.empty_cache()
     out = {'tunnels': len(solvers), 'cells': cells, 'tile': tile,
            'tile_ms_per_step': {str(a): round(v, 3) for a, v in tile_ms.items()},
            'graph_steps': graph_steps, 'replays': replays, 'ms_per_step': round(t / (replays * graph_steps) * 1e3, 4),
            'glups': round(cells * replays * graph_steps / t / 1e9, 3),
            'streams': {'ms_per_step': round(ts / (replays * graph_steps) * 1e3, 4),
                        'glups': round(cells * replays * graph_steps / ts / 1e9, 3)},
-           'checked_tunnel': list(dims), 'checked_steps': steps_done, 'bit_identical_to_alone': same}
-    del solvers, alone
+           'alone_sequential_glups': round(cells * steps_done / alone_s / 1e9, 3),
+           'checked_steps': steps_done, 'tunnels_bit_identical_to_alone': sum(r['bit_identical'] for r in per),
+           'per_tunnel': per}
+    del solvers
     torch.cuda.empty_cache()
     return out
 

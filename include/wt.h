@@ -152,12 +152,13 @@ int wt_forces_noalloc(const wt_grid* g, int32_t cur, const int32_t* cells, const
 int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void* stream);
 
 /* ---- many tunnels at once ----
- * A batch advances `count` tunnels of uneven sizes together: per step one persistent bulk
- * kernel over a tile work-list spanning all tunnels, then one kernel over all tunnels' face
- * cells. No counterpart in the reference, which runs one tunnel (server/app.py:116); each
- * tunnel's results are bit-identical to stepping it alone with wt_step. All tunnels share
- * precision and collision form; tile is a direct-load tile id of wt_step_tiles (0 =
- * default). The caller allocates a 256-byte aligned device workspace of
+ * A batch advances `count` tunnels of uneven sizes together: per step one bulk kernel over a
+ * tile work-list spanning all tunnels, then one kernel over all tunnels' face cells. No
+ * counterpart in the reference, which runs one tunnel (server/app.py:116); each tunnel's
+ * results are bit-identical to stepping it alone with wt_step. All tunnels share precision and
+ * collision form. tile selects the shape: a direct-load tile id k of wt_step_tiles (1-5, 7, 18)
+ * runs as a persistent kernel (one wave of blocks looping over the work list); 100 + k (102,
+ * 103, 104, 118) as one block per work-list tile; 0 = default. The caller allocates a 256-byte aligned device workspace of
  * wt_batch_workspace_bytes (descriptor table and work lists). cur gives each tunnel's
  * current population buffer at creation; wt_batch_cur reports it later. A batch must be
  * re-created after any of its tunnels is stepped on its own. */

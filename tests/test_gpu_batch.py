@@ -32,7 +32,7 @@ def _alone(dims, solid, p, steps, collision, precision):
 
 
 @pytest.mark.parametrize('collision,precision', [('exact', 'fp32'), ('fast', 'fp16')])
-@pytest.mark.parametrize('tile', [2, 3])
+@pytest.mark.parametrize('tile', [2, 3, 102, 118])
 def test_batch_equals_tunnels_alone(collision, precision, tile):
     from batch import TunnelBatch
     tun = _tunnels(collision, precision)

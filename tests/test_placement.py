@@ -103,6 +103,9 @@ class _FakeSolver:
     def launch_frame_packed(self, p, want_cp):
         pass
 
+    def frame_ready(self):
+        return True
+
     def collect_frame_packed(self, header):
         return b'frame'
 

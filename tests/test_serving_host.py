@@ -53,6 +53,9 @@ class FakeSolver:
         if want_cp:
             self.cp_frames.append(self.launched)
 
+    def frame_ready(self):
+        return True
+
     def collect_frame_packed(self, header):
         return repr((self.s.id, self.launched, sorted(header))).encode()
 
@@ -407,3 +410,50 @@ def test_command_arriving_during_a_drain_waits_for_the_next_round():
     c.t += 1 / 30
     srv.round()
     assert [k for k, _ in sv.calls] == ['reset', 'set_particles']
+
+
+def test_admission_worker_builds_tunnels_while_rounds_run():
+    """With admit_thread the tunnels are built on a worker thread: a session joins the first
+    round after its tunnel is ready, its memory is reserved from dispatch on, and commands sent
+    while it is being built are applied, in order, once it is active."""
+    import threading
+    import time
+    c = Clock()
+    gate = threading.Event()
+
+    def factory(s):
+        if s.id == 1:
+            raise MemoryError('out of memory')
+        if s.id == 2:
+            gate.wait(10)  # session 2's tunnel takes a while
+        return FakeSolver(s)
+    srv = serving.SessionServer(device=None, budget_bytes=100, clock=c, solver_factory=factory,
+                                batch_factory=lambda sv, p: FakeBatch(c, 1e12, sv), footprint=lambda s: float(s.n),
+                                admit_thread=True)
+    try:
+        for i in range(3):
+            srv.submit(_session(i, 4))
+        srv.round()
+        assert srv.used == 12 and set(srv.building) <= {0, 1, 2}
+        srv.command(2, {'type': 'params', 'tau': 0.7})
+        srv.command(2, {'type': 'respawn'})
+        for _ in range(200):  # session 0 is built at once, 1 fails, 2 waits for the gate
+            c.t += 1 / 30
+            srv.round()
+            if 0 in srv.active and srv.failed:
+                break
+            time.sleep(0.005)
+        assert 0 in srv.active and 2 in srv.building and srv.active[0].frames >= 1
+        assert srv.failed == 1 and 'Could not allocate' in srv.errors[0][1] and srv.used == 8
+        gate.set()
+        for _ in range(200):
+            c.t += 1 / 30
+            srv.round()
+            if 2 in srv.active:
+                break
+            time.sleep(0.005)
+        s2 = srv.active[2]
+        assert s2.p['tau'] == 0.7 and s2.solver.calls == [('set_particles', 7)]
+    finally:
+        gate.set()
+        srv.close()

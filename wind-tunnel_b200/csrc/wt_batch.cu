@@ -1,15 +1,19 @@
-// Many tunnels of uneven sizes advanced together: one persistent bulk kernel over a tile
-// work-list spanning every tunnel, then one face kernel over all tunnels' face cells, per
-// step; optionally captured as a CUDA graph of an even number of steps and replayed.
+// Many tunnels of uneven sizes advanced together: one bulk kernel over a tile work-list
+// spanning every tunnel, then one face kernel over all tunnels' face cells, per step; optionally
+// captured as a CUDA graph of an even number of steps and replayed. The kernels come in two
+// forms (wt_kernels.cuh): persistent (one wave of blocks looping over the lists) and grid (one
+// block per sub-tile of the lists, tile ids 100 + k), which fits the 64 registers of the
+// single-tunnel two-cell tile.
 //
 // Device workspace (caller-allocated, wt_batch_workspace_bytes):
 //   desc  -- 4 StepArgs per tunnel, indexed [tunnel][parity][mac_all]: parity p holds the
 //            tunnel's buffers for cur = cur0 ^ p, so all tunnels flip together;
 //   bulk  -- work items {tunnel, first cell} of BLOCK * V * ITEM_SUB cells each;
 //   faces -- work items {tunnel, first face index} of FACE_BLOCK * ITEM_SUB face cells each.
-// Each CTA copies the descriptor of its current item into shared memory, so the kernel body
-// is the single-tunnel one (bulk_cells / face_cell of wt_step_impl.cuh) and every tunnel
-// gives bit-identical results alone or in a batch. The kernels (k_batch_bulk, k_batch_faces)
+// A persistent block copies the descriptor of its current item into shared memory; a grid-form
+// block reads it in place. Either way the kernel body is the single-tunnel one (bulk_cells /
+// face_cell of wt_step_impl.cuh) and every tunnel gives bit-identical results alone or in a
+// batch. The kernels (k_batch_bulk, k_batch_faces)
 // are instantiated per precision in wt_kernels_<prec>.cu; this file is the host side.
 #include <cstring>
 #include <vector>
@@ -52,10 +56,11 @@ size_t desc_bytes_for(int32_t precision) {
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
-// tile shape of a batch (direct-load variants only)
+// tile shape of a batch (direct-load variants only; 100 + k is the grid form of tile k)
 int tile_shape(int32_t tile, int* v, int* block) {
-    static const int ids[][3] = {{1, 1, 256}, {2, 1, 128}, {3, 2, 128}, {4, 2, 128}, {5, 4, 128}, {7, 2, 256},
-                                 {18, 2, 128}};
+    static const int ids[][3] = {{1, 1, 256},   {2, 1, 128},   {3, 2, 128},   {4, 2, 128},  {5, 4, 128},
+                                 {7, 2, 256},   {18, 2, 128},  {102, 1, 128}, {103, 2, 128}, {104, 2, 128},
+                                 {118, 2, 128}};
     const int want = tile > 0 ? tile : 2;
     for (const auto& r : ids)
         if (r[0] == want) {
@@ -219,8 +224,13 @@ extern "C" int wt_batch_create(const wt_grid* grids, int32_t count, const double
     b->faces = reinterpret_cast<int2*>(static_cast<unsigned char*>(workspace) + align256(4 * ds * count) + align256(8 * nb));
     b->n_bulk = (int32_t)nb;
     b->n_faces = (int32_t)nf;
-    b->grid_bulk = (int)std::min<int64_t>(nb, (int64_t)num_sms() * var->minb);  // persistent: one wave
-    b->grid_faces = (int)std::min<int64_t>(nf, (int64_t)num_sms() * 8);
+    if (var->persistent) {  // one wave of blocks looping over the lists
+        b->grid_bulk = (int)std::min<int64_t>(nb, (int64_t)num_sms() * var->minb);
+        b->grid_faces = (int)std::min<int64_t>(nf, (int64_t)num_sms() * 8);
+    } else {  // one block per sub-tile
+        b->grid_bulk = (int)(nb * ITEM_SUB);
+        b->grid_faces = (int)(nf * ITEM_SUB);
+    }
     b->graph = nullptr;
     b->graph_steps = 0;
     *out = b;

@@ -60,6 +60,34 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     return WT_OK;
 }
 
+template <int PREC, bool FAST, int BLOCK, int MINB, int ROWS>
+static int launch_pipe(const void* args, int32_t n, cudaStream_t st) {
+    using P = Prec<PREC>;
+    using S = typename P::S;
+    using T = typename P::T;
+    (void)n;
+    RowArgs<S, T> r;
+    r.a = *static_cast<const StepArgs<S, T>*>(args);
+    const StepArgs<S, T>& a = r.a;
+    for (int i = 0; i < Q; ++i) {
+        r.loff[i] = ((int64_t)i * a.n - (int64_t)cy(i) * a.nx - (int64_t)cz(i) * a.nxy) * (int64_t)sizeof(S);
+        r.soff[i] = (int64_t)i * a.n * (int64_t)sizeof(S);
+    }
+    static bool configured = false;
+    if (!configured) {  // MINB blocks of double-buffered stages need most of the SM's shared memory
+        if (cudaFuncSetAttribute(k_step_pipe<PREC, FAST, BLOCK, MINB, ROWS>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
+            return wt_cuda_check("wt_step: shared-memory carve-out");
+        configured = true;
+    }
+    const int32_t nrows = a.ny * a.nz;
+    k_step_pipe<PREC, FAST, BLOCK, MINB, ROWS><<<(unsigned)((nrows + ROWS - 1) / ROWS), BLOCK, 0, st>>>(r);
+    // then every pair the pipelined kernel leaves (tile 19's shape)
+    const dim3 grid((unsigned)((a.nx / 2 + 127) / 128), (unsigned)a.ny, (unsigned)a.nz);
+    k_step_rows<PREC, FAST, 128, 8, 0, true><<<grid, 128, 0, st>>>(r);
+    return WT_OK;
+}
+
 // Tile variants. Direct-load forms (kind 0): cells per thread (V), threads per block, minimum
 // resident blocks per SM. Streaming forms (kind 1): chunk length L, pipeline stages NS,
 // threads per block, blocks per SM. Row-grid forms (kind 2, k_step_rows): two cells per
@@ -94,11 +122,25 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     {25, 2, 2, 128, 9, 0, 0, launch_rows<PREC, FAST, 128, 9, 0>},                        \
     {26, 2, 2, 128, 10, 0, 0, launch_rows<PREC, FAST, 128, 10, 0>}
 
+// pipelined row forms (kind 3, k_step_pipe, half-width storage only): two cells per thread,
+// threads per block, resident blocks per SM, and in the last field the rows per block
+#define WT_VARIANTS_HALF(PREC, FAST)                                                     \
+    {27, 3, 2, 128, 7, 0, 4, launch_pipe<PREC, FAST, 128, 7, 4>},                        \
+    {28, 3, 2, 128, 7, 0, 8, launch_pipe<PREC, FAST, 128, 7, 8>},                        \
+    {29, 3, 2, 64, 14, 0, 4, launch_pipe<PREC, FAST, 64, 14, 4>},                        \
+    {30, 3, 2, 128, 7, 0, 16, launch_pipe<PREC, FAST, 128, 7, 16>}
+
 template <int PREC, bool FAST>
 const StepVariant* variants_of(int* count) {
-    static const StepVariant table[] = {WT_VARIANTS(PREC, FAST)};
-    *count = (int)(sizeof(table) / sizeof(table[0]));
-    return table;
+    if constexpr (sizeof(typename Prec<PREC>::S) == 2) {
+        static const StepVariant table[] = {WT_VARIANTS(PREC, FAST), WT_VARIANTS_HALF(PREC, FAST)};
+        *count = (int)(sizeof(table) / sizeof(table[0]));
+        return table;
+    } else {
+        static const StepVariant table[] = {WT_VARIANTS(PREC, FAST)};
+        *count = (int)(sizeof(table) / sizeof(table[0]));
+        return table;
+    }
 }
 
 template <int PREC>
@@ -222,6 +264,39 @@ __global__ void __launch_bounds__(FACE_BLOCK) k_batch_faces(const BatchArgs b) {
     }
 }
 
+// Grid forms of the same two kernels: one block per sub-tile of the work list (block b: item
+// b / ITEM_SUB, sub-tile b % ITEM_SUB), the descriptor read in place from the workspace. With no
+// loop over items the compiler keeps no descriptor field in a register across tiles, so the
+// two-cell tile fits the 64 registers of the single-tunnel tile 18 (the persistent loop above
+// needs 80, or spills).
+template <int PREC, bool FAST, int V, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_batch_bulk_grid(const BatchArgs b) {
+    using A = StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>;
+    const int32_t w = (int32_t)blockIdx.x / ITEM_SUB, sub = (int32_t)blockIdx.x % ITEM_SUB;
+    const int2 item = b.bulk[w];
+    const A* __restrict__ a = static_cast<const A*>(b.desc) + item.x * 4 + b.parity * 2 + b.mac_all;
+    const int32_t idx0 = item.y + (sub * BLOCK + (int32_t)threadIdx.x) * V;
+    bulk_cells<PREC, FAST, V>(*a, idx0, idx0 < a->n);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(FACE_BLOCK) k_batch_faces_grid(const BatchArgs b) {
+    using A = StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>;
+    const int32_t w = (int32_t)blockIdx.x / ITEM_SUB, sub = (int32_t)blockIdx.x % ITEM_SUB;
+    const int2 item = b.faces[w];
+    const A* __restrict__ a = static_cast<const A*>(b.desc) + item.x * 4 + b.parity * 2 + b.mac_all;
+    face_cell<PREC>(*a, item.y + sub * FACE_BLOCK + (int32_t)threadIdx.x);
+}
+
+template <int PREC, bool FAST, int V, int BLOCK, int MINB>
+static void launch_batch_bulk_grid(const void* args, int grid, cudaStream_t st) {
+    k_batch_bulk_grid<PREC, FAST, V, BLOCK, MINB><<<grid, BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
+}
+template <int PREC>
+static void launch_batch_faces_grid(const void* args, int grid, cudaStream_t st) {
+    k_batch_faces_grid<PREC><<<grid, FACE_BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
+}
+
 template <int PREC, bool FAST, int V, int BLOCK, int MINB>
 static void launch_batch_bulk(const void* args, int grid, cudaStream_t st) {
     k_batch_bulk<PREC, FAST, V, BLOCK, MINB><<<grid, BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
@@ -231,15 +306,20 @@ static void launch_batch_faces(const void* args, int grid, cudaStream_t st) {
     k_batch_faces<PREC><<<grid, FACE_BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
 }
 
-// the direct-load tile shapes of wt_step, same ids
+// the direct-load tile shapes of wt_step, same ids, as persistent kernels; ids 100 + k are
+// the grid forms of tile k
 #define WT_BATCH_VARIANTS(PREC, FAST)                                                                        \
-    {1, 1, 256, 4, launch_batch_bulk<PREC, FAST, 1, 256, 4>, launch_batch_faces<PREC>},                      \
-    {2, 1, 128, 8, launch_batch_bulk<PREC, FAST, 1, 128, 8>, launch_batch_faces<PREC>},                      \
-    {3, 2, 128, 6, launch_batch_bulk<PREC, FAST, 2, 128, 6>, launch_batch_faces<PREC>},                      \
-    {4, 2, 128, 4, launch_batch_bulk<PREC, FAST, 2, 128, 4>, launch_batch_faces<PREC>},                      \
-    {5, 4, 128, 4, launch_batch_bulk<PREC, FAST, 4, 128, 4>, launch_batch_faces<PREC>},                      \
-    {7, 2, 256, 3, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>},                      \
-    {18, 2, 128, 8, launch_batch_bulk<PREC, FAST, 2, 128, 8>, launch_batch_faces<PREC>}
+    {1, 1, 256, 4, true, launch_batch_bulk<PREC, FAST, 1, 256, 4>, launch_batch_faces<PREC>},                \
+    {2, 1, 128, 8, true, launch_batch_bulk<PREC, FAST, 1, 128, 8>, launch_batch_faces<PREC>},                \
+    {3, 2, 128, 6, true, launch_batch_bulk<PREC, FAST, 2, 128, 6>, launch_batch_faces<PREC>},                \
+    {4, 2, 128, 4, true, launch_batch_bulk<PREC, FAST, 2, 128, 4>, launch_batch_faces<PREC>},                \
+    {5, 4, 128, 4, true, launch_batch_bulk<PREC, FAST, 4, 128, 4>, launch_batch_faces<PREC>},                \
+    {7, 2, 256, 3, true, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>},                \
+    {18, 2, 128, 8, true, launch_batch_bulk<PREC, FAST, 2, 128, 8>, launch_batch_faces<PREC>},               \
+    {102, 1, 128, 8, false, launch_batch_bulk_grid<PREC, FAST, 1, 128, 8>, launch_batch_faces_grid<PREC>},   \
+    {103, 2, 128, 6, false, launch_batch_bulk_grid<PREC, FAST, 2, 128, 6>, launch_batch_faces_grid<PREC>},   \
+    {104, 2, 128, 4, false, launch_batch_bulk_grid<PREC, FAST, 2, 128, 4>, launch_batch_faces_grid<PREC>},   \
+    {118, 2, 128, 8, false, launch_batch_bulk_grid<PREC, FAST, 2, 128, 8>, launch_batch_faces_grid<PREC>}
 
 template <int PREC, bool FAST>
 const BatchVariant* batch_variant_of(int id) {

@@ -1084,6 +1084,11 @@ struct RowArgs {
     int64_t soff[Q];  // bytes from fout + idx0 to population i of the output
 };
 
+template <int PREC, bool FAST>
+__device__ __forceinline__ void pair_lean_finish(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
+                                                 typename Prec<PREC>::T (&f)[2][Q], int32_t idx0, int32_t x0,
+                                                 int32_t y, int32_t z, uint32_t codes, bool row_shell, bool offs);
+
 template <int PREC, bool FAST, int ADDR>
 __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
                                           int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
@@ -1092,7 +1097,6 @@ __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, 
     using S = typename P::S;
     using T = typename P::T;
     const auto& a = r.a;
-    const int32_t nx = a.nx;
     const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * (int64_t)sizeof(S);
     T f[2][Q];
     unroll<0, Q>([&](auto ic) {
@@ -1114,6 +1118,19 @@ __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, 
             f[1][i] = ld_in<P, FAST, i>(a, p + 2);
         }
     });
+    pair_lean_finish<PREC, FAST>(r, f, idx0, x0, y, z, codes, row_shell, ADDR == 1);
+}
+
+// The lean path after the pull: walls, collision, inlet / outlet, stores and mac (see k_step_rows).
+template <int PREC, bool FAST>
+__device__ __forceinline__ void pair_lean_finish(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
+                                                 typename Prec<PREC>::T (&f)[2][Q], int32_t idx0, int32_t x0,
+                                                 int32_t y, int32_t z, uint32_t codes, bool row_shell, bool offs) {
+    using P = Prec<PREC>;
+    using S = typename P::S;
+    using T = typename P::T;
+    const auto& a = r.a;
+    const int32_t nx = a.nx;
     const uint32_t c0 = codes & 0xffu, c1 = codes >> 8;
     if ((c0 | c1) & CODE_NEAR) pair_walls<PREC, FAST>(a, idx0, c0, c1, f);  // lanes next to a wall
     T m[2][4];
@@ -1131,7 +1148,7 @@ __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, 
     char* ob = reinterpret_cast<char*>(a.dst[0]) + (int64_t)idx0 * (int64_t)sizeof(S);
     unroll<0, Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        store_cells<P, FAST, 2, i>(a, ADDR == 0 ? a.dst[i] + idx0 : reinterpret_cast<S*>(ob + r.soff[i]), f);
+        store_cells<P, FAST, 2, i>(a, offs ? reinterpret_cast<S*>(ob + r.soff[i]) : a.dst[i] + idx0, f);
     });
     // mac where faces read it (coordinates 1 and n-2), and everywhere when mac_all
     const bool w0 = a.mac_all || (!inlet && (row_shell || x0 == nx - 2));
@@ -1140,7 +1157,12 @@ __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, 
     if (w1) store_mac(a.mac_cur, idx0 + 1, m[1][0], m[1][1], m[1][2], m[1][3]);
 }
 
-template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR>
+// the pure-pair test both kernels apply (codes: the pair's two code bytes)
+__device__ __forceinline__ bool pure_pair(bool interior_row, bool valid, uint32_t codes, int32_t x0, int32_t nx) {
+    return interior_row && valid && codes == 0 && x0 > 0 && x0 + 2 < nx;
+}
+
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool SKIP_PURE = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
     const auto& a = r.a;
     const int32_t y = (int32_t)blockIdx.y, z = (int32_t)blockIdx.z;
@@ -1154,11 +1176,148 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typenam
     }
     const bool row_shell = y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2;
     const uint32_t codes = valid ? *reinterpret_cast<const uint16_t*>(a.code + idx0) : 0xffffu;
+    if constexpr (SKIP_PURE) {  // k_step_pipe has computed the pure pairs
+        const bool todo = valid && !pure_pair(true, valid, codes, x0, nx);
+        if (!__any_sync(0xffffffffu, todo)) return;
+        if (__all_sync(0xffffffffu, !todo || (codes & (CODE_SOLID * 0x0101u)) == 0)) {
+            if (todo) pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell);
+        } else if (todo) {
+            interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell);
+        }
+        return;
+    }
     // lean unless a cell of the warp is solid (or past the row's end)
     if (__all_sync(0xffffffffu, (codes & (CODE_SOLID * 0x0101u)) == 0)) {
         pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell);
     } else if (valid) {
         interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Pipelined row form for half-width storage (fp16 / bf16). The row kernel above waits on its
+// loads with one pair per thread in flight (64 registers hold one pair), so the step is bound
+// by load latency, not by HBM or issue. Here the work of a step is split in two kernels:
+//
+// * k_step_pipe computes every PURE pair: both cells plain interior fluid (code 0) in an
+//   interior row, neither the inlet nor the outlet pair. Each block walks ROWS lattice rows
+//   (items: the rows' x-runs of 2 * BLOCK cells) and every thread stages the pull of its NEXT
+//   item into shared memory with per-thread asynchronous copies (cp.async, 4 bytes each: the
+//   19 aligned pairs, the 10 pairs holding the x-shifted neighbours, the code word) while it
+//   computes the current one from the previous stage. The stage is double-buffered and each
+//   thread reads only the words it copied itself, so no block barrier is needed: the copies of
+//   item j + 1 go to the buffer of item j - 1, whose words this thread consumed in iteration
+//   j - 1. Its loop body is the pure path alone, which keeps every kernel parameter it does not
+//   need out of registers (a loop over the general paths spills).
+// * k_step_rows with SKIP_PURE then computes the rest (face rows, the inlet and outlet pairs,
+//   pairs next to walls or holding a solid cell) and leaves the pure pairs alone. Both decide
+//   purity by the same per-pair test, so every cell is written exactly once, by the same
+//   arithmetic as the other two-cell tiles: the results are bit for bit theirs.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+constexpr int PIPE_WORDS = Q + 10;  // 19 aligned pairs, then the neighbour pairs of cx != 0
+
+template <int PREC, bool FAST, int BLOCK, int MINB, int ROWS>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_step_pipe(const __grid_constant__ RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
+    using P = Prec<PREC>;
+    using S = typename P::S;
+    using T = typename P::T;
+    static_assert(sizeof(S) == 2, "the pipelined tile stages pairs of half-width values as 4-byte words");
+    __shared__ uint32_t stage[2][PIPE_WORDS][BLOCK];
+    __shared__ uint32_t stage_code[2][BLOCK];
+    const auto& a = r.a;
+    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
+    const int32_t tid = (int32_t)threadIdx.x;
+    const int32_t xruns = (nx / 2 + BLOCK - 1) / BLOCK;
+    const int32_t row0 = (int32_t)blockIdx.x * ROWS;
+    const int32_t items = min(ROWS, ny * nz - row0) * xruns;
+    // item j: row row0 + j / xruns, pair x0 = 2 (BLOCK (j % xruns) + tid)
+    auto place = [&](int32_t j, int32_t& row, int32_t& x0, int32_t& y, int32_t& z) {
+        const int32_t rr = j / xruns;
+        row = row0 + rr;
+        x0 = ((j - rr * xruns) * BLOCK + tid) * 2;
+        z = (int32_t)a.dny.div((uint32_t)row);
+        y = row - z * ny;
+    };
+    auto issue = [&](int32_t j) {  // stage item j's pull into buffer j & 1 (pairs that may be pure)
+        if (j >= items) return;
+        int32_t row, x0, y, z;
+        place(j, row, x0, y, z);
+        if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1 || x0 == 0 || x0 + 2 >= nx) return;
+        const int32_t idx0 = x0 + row * nx;
+        const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * 2;
+        const int b = j & 1;
+        int k = Q;
+        // offsets read afresh for every item (a volatile read of the grid constant)
+        const volatile int64_t* loff = r.loff;
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            const char* w = fb + loff[i];  // the aligned pair (x0, x0 + 1) of the source row
+            cp_async4(&stage[b][i][tid], w);
+            // the pair holding x0 - 1 (cx > 0) or x0 + 2 (cx < 0), inside the source row
+            // (0 < x0 < nx - 2)
+            if constexpr (cx(i) > 0) cp_async4(&stage[b][k++][tid], w - 4);
+            if constexpr (cx(i) < 0) cp_async4(&stage[b][k++][tid], w + 4);
+        });
+        cp_async4(&stage_code[b][tid], a.code + (idx0 & ~3));
+    };
+    issue(0);
+    cp_async_commit();
+#pragma unroll 1
+    for (int32_t j = 0; j < items; ++j) {
+        issue(j + 1);
+        cp_async_commit();
+        cp_async_wait1();  // this thread's copies of item j have landed
+        int32_t row, x0, y, z;
+        place(j, row, x0, y, z);
+        const bool interior_row = !(y == 0 || y == ny - 1 || z == 0 || z == nz - 1);
+        const bool staged = interior_row && x0 > 0 && x0 + 2 < nx;
+        const int b = j & 1;
+        const int32_t idx0 = x0 + row * nx;
+        const uint32_t codes = staged ? (stage_code[b][tid] >> (8 * (idx0 & 3))) & 0xffffu : 0xffffu;
+        if (!pure_pair(interior_row, staged, codes, x0, nx)) continue;  // left to k_step_rows
+        T f[2][Q];
+        int k = Q;
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            S v[2], e[2];
+            const uint32_t w = stage[b][i][tid];
+            memcpy(v, &w, 4);
+            if constexpr (cx(i) == 0) {
+                f[0][i] = ld_in<P, FAST, i>(a, &v[0]);
+                f[1][i] = ld_in<P, FAST, i>(a, &v[1]);
+            } else {
+                const uint32_t wn = stage[b][k++][tid];
+                memcpy(e, &wn, 4);
+                if constexpr (cx(i) > 0) {
+                    f[0][i] = ld_in<P, FAST, i>(a, &e[1]);  // x0 - 1
+                    f[1][i] = ld_in<P, FAST, i>(a, &v[0]);
+                } else {
+                    f[0][i] = ld_in<P, FAST, i>(a, &v[1]);
+                    f[1][i] = ld_in<P, FAST, i>(a, &e[0]);  // x0 + 2
+                }
+            }
+        });
+        T m[2][4];
+        collide_two<P, FAST>(a, f, x0, m);
+        char* ob = reinterpret_cast<char*>(a.dst[0]) + (int64_t)idx0 * (int64_t)sizeof(S);
+        const volatile int64_t* soff = r.soff;
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            store_cells<P, FAST, 2, i>(a, reinterpret_cast<S*>(ob + soff[i]), f);
+        });
+        // mac where faces read it: a pure pair holds neither x = 1 nor x = nx - 2
+        if (a.mac_all || y == 1 || y == ny - 2 || z == 1 || z == nz - 2) {
+            store_mac(a.mac_cur, idx0, m[0][0], m[0][1], m[0][2], m[0][3]);
+            store_mac(a.mac_cur, idx0 + 1, m[1][0], m[1][1], m[1][2], m[1][3]);
+        }
     }
 }
 

@@ -18,9 +18,11 @@ struct StepVariant {
     int (*launch)(const void* args, int32_t n, cudaStream_t st);
 };
 
-// One tile shape of the batched bulk kernel and its face kernel.
+// One tile shape of the batched bulk kernel and its face kernel. persistent: a grid of one
+// wave whose blocks loop over the work list; otherwise one block per sub-tile of the list.
 struct BatchVariant {
     int id, v, block, minb;
+    bool persistent;
     void (*bulk)(const void* args, int grid, cudaStream_t st);
     void (*faces)(const void* args, int grid, cudaStream_t st);
 };

@@ -372,6 +372,10 @@ class Solver:
             self._pk_event.record(self.stream)
         self._pk_pending = (layout, extra)
 
+    def frame_ready(self):
+        """True once launch_frame_packed's copy has landed (collect_frame_packed will not wait)."""
+        return self._pk_pending is None or self._pk_event.query()
+
     def collect_frame_packed(self, header):
         """Wait for launch_frame_packed's copy and return the frame bytes. ``header`` holds
         the Engine's keys in its order (type, dims, numP, numVerts, forces, steps, mlups,

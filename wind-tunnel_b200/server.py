@@ -181,7 +181,8 @@ def main(argv=None):
     ap.add_argument('--device', default='cuda:0')
     a = ap.parse_args(argv)
     import torch
-    srv = serving.SessionServer(a.device, budget_bytes=a.budget_gb * 1e9, precision=a.precision, pacing='client')
+    srv = serving.SessionServer(a.device, budget_bytes=a.budget_gb * 1e9, precision=a.precision, pacing='client',
+                                admit_thread=True)
     name = torch.cuda.get_device_name(torch.device(a.device))
     web.run_app(make_app(srv, name, int(a.budget_gb * 1e9)), host=a.host, port=a.port, print=None)
 

@@ -90,6 +90,8 @@ class Session:
         self.ready = True          # client pacing: the client holds no unacknowledged frame
         self.verts = self.norms = None  # surface points for Cp, once uploaded
         self.applied = []          # (frames before it, message, payload) per command, with keep_frames
+        self.deferred = []         # commands that arrived while its tunnel was being built
+        self.demand = 0.0          # lattice updates per second it requests (admission's work bound)
 
     @property
     def running(self):
@@ -107,7 +109,7 @@ class SessionServer:
     def __init__(self, device='cuda:0', budget_bytes=160e9, precision='fp32', fps=30.0, steps_per_frame=10,
                  tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
                  footprint=None, keep_frames=False, batch_mode='streams', pacing='fps', paused_hz=PAUSED_HZ,
-                 rate_in_header=True):
+                 rate_in_header=True, priorities=True, work_bound_glups=None, admit_thread=False):
         self.device = device
         self.budget = float(budget_bytes)
         self.precision = precision
@@ -133,6 +135,24 @@ class SessionServer:
         self.pacing = pacing
         self.paused_period = 1.0 / paused_hz
         self.rate_in_header = rate_in_header
+        # streams executor: each session's stream gets a CUDA priority by tunnel size, smaller
+        # tunnels higher, so within a round their few blocks are scheduled ahead of the big
+        # tunnels' and their frames finish early; every session still gets one frame per round
+        self.priorities = priorities
+        # opt-in admission bound on requested work: admit a session only while the lattice
+        # updates per second that every admitted session requests (cells x steps per frame x
+        # fps) stay within work_bound_glups; None admits by the HBM budget alone
+        self.work_bound = None if work_bound_glups is None else float(work_bound_glups) * 1e9
+        self.demand = 0.0
+        # admit_thread: a worker thread builds admitted sessions' tunnels (allocation, mask
+        # upload, link list, particles, pinned frame buffers) while rounds run; a session joins
+        # the first round after its tunnel is ready, and commands sent meanwhile wait for it.
+        # Without it (the default) admission builds the tunnel inside the round.
+        self.building = {}                  # id -> Session whose tunnel the worker is building
+        self._built = collections.deque()   # (session, exception or None) the worker finished
+        self._jobs = None
+        if admit_thread:
+            self._start_worker()
         # (session id, message, payload) in arrival order; a deque, so the front end's threads
         # can append while the serving thread drains (the reference's handlers feed its Engine
         # through a queue the same way, server/app.py:212-222)
@@ -161,9 +181,39 @@ class SessionServer:
         self.step_gpu_s = 0.0  # device time of the batched steps (CUDA events on the batch stream)
         self.step_cells = 0
 
+    def _start_worker(self):
+        import queue
+        import threading
+        self._jobs = queue.Queue()
+
+        def work():
+            if self.device is not None:
+                import torch
+                torch.cuda.set_device(torch.device(self.device))
+            while True:
+                s = self._jobs.get()
+                if s is None:
+                    return
+                try:
+                    s.solver, err = self.solver_factory(s), None
+                except Exception as e:  # reported by the serving thread (server/app.py:115-122)
+                    s.solver, err = None, e
+                self._built.append((s, err))
+        self._worker = threading.Thread(target=work, name='admission', daemon=True)
+        self._worker.start()
+
     # ---- default factories (the GPU path) ----
+    def _priority(self, s):
+        """CUDA stream priority of a session (lower is higher): smaller tunnels first."""
+        if not self.priorities or self.batch_mode != 'streams':
+            return 0
+        return -3 if s.n <= 1_000_000 else (-2 if s.n <= 4_000_000 else (-1 if s.n <= 16_000_000 else 0))
+
     def _make_solver(self, s):
-        sv = lbm.Solver(s.dims, self.device, precision=self.precision, collision=self.collision, seed=s.id)
+        import torch
+        stream = torch.cuda.Stream(torch.device(self.device), priority=self._priority(s))
+        sv = lbm.Solver(s.dims, self.device, precision=self.precision, collision=self.collision, seed=s.id,
+                        stream=stream)
         sv.set_solid(s.solid)
         sv.reset(s.p['uIn'])
         if s.particles:
@@ -221,6 +271,9 @@ class SessionServer:
             if msg is _SUBMIT:
                 self.submit(payload)
                 continue
+            if sid in self.building:  # its tunnel is being built: applied once it is active
+                self.building[sid].deferred.append((msg, payload))
+                continue
             s = self.active.get(sid)
             if s is None:
                 s = next((q for q in self.queue if q.id == sid), None)
@@ -230,15 +283,18 @@ class SessionServer:
                 if msg is not None:
                     self.errors.append((sid, f"command {msg.get('type')!r} for no session"))
                 continue
-            if msg is None:  # disconnected: the lifetime ends now (retired or abandoned below)
-                s.lifetime = min(s.lifetime, now - s.arrival)
-                continue
-            if self.keep_frames:  # which frames each command came before (test replays)
-                s.applied.append((s.frame_no, dict(msg), payload))
-            try:
-                self._apply(s, msg, payload, now)
-            except Exception as e:  # a bad message fails alone (the Engine reports it, server/app.py:160-161)
-                self.errors.append((sid, f'command failed: {e!r}'))
+            self._apply_one(s, msg, payload, now)
+
+    def _apply_one(self, s, msg, payload, now):
+        if msg is None:  # disconnected: the lifetime ends now (retired or abandoned)
+            s.lifetime = min(s.lifetime, now - s.arrival)
+            return
+        if self.keep_frames:  # which frames each command came before (test replays)
+            s.applied.append((s.frame_no, dict(msg), payload))
+        try:
+            self._apply(s, msg, payload, now)
+        except Exception as e:  # a bad message fails alone (the Engine reports it, server/app.py:160-161)
+            self.errors.append((s.id, f'command failed: {e!r}'))
 
     def _apply(self, s, msg, payload, now):
         t = msg.get('type')
@@ -314,7 +370,29 @@ class SessionServer:
         command sent right after enqueue() finds its session."""
         self._cmds.append((session.id, _SUBMIT, session))
 
+    def _activate(self, s, now):
+        s.bytes = max(s.bytes, s.solver.device_bytes())
+        s.admitted_t = s.request_t = s.last_t = now
+        self.active[s.id] = s
+        self.admitted += 1
+
     def _admit(self, now):
+        while self._built:  # tunnels the worker finished join this round
+            s, err = self._built.popleft()
+            del self.building[s.id]
+            if err is not None:
+                self.used -= s.bytes
+                self.demand -= s.demand
+                self.failed += 1
+                self.errors.append((s.id, f'Could not allocate {"x".join(map(str, s.dims))} grid: {err}'))
+                continue
+            self.used -= s.bytes
+            self._activate(s, now)
+            self.used += s.bytes
+            self.peak_used = max(self.peak_used, self.used)
+            for msg, payload in s.deferred:  # commands sent while it was being built
+                self._apply_one(s, msg, payload, now)
+            s.deferred = []
         while self.queue:
             s = self.queue[0]
             if now - s.arrival >= s.lifetime:  # the client gave up while waiting
@@ -324,7 +402,19 @@ class SessionServer:
             need = self.footprint(s)
             if self.used + need > self.budget:
                 break
+            want = self._demand(s)
+            if self.work_bound is not None and self.active and self.demand + want > self.work_bound:
+                break
             self.queue.pop(0)
+            s.demand = want
+            if self._jobs is not None:  # built by the worker; memory and demand reserved now
+                s.bytes = need
+                self.used += need
+                self.demand += want
+                self.peak_used = max(self.peak_used, self.used)
+                self.building[s.id] = s
+                self._jobs.put(s)
+                continue
             try:
                 s.solver = self.solver_factory(s)
             except Exception as e:  # out of memory etc. (server/app.py:115-122)
@@ -332,13 +422,16 @@ class SessionServer:
                 self.failed += 1
                 self.errors.append((s.id, f'Could not allocate {"x".join(map(str, s.dims))} grid: {e}'))
                 continue
-            s.bytes = max(need, s.solver.device_bytes())
-            s.admitted_t = s.request_t = s.last_t = now
+            s.bytes = need
+            self._activate(s, now)
+            self.demand += want
             self.used += s.bytes
             self.peak_used = max(self.peak_used, self.used)
-            self.active[s.id] = s
-            self.admitted += 1
         self.max_active = max(self.max_active, len(self.active))
+
+    def _demand(self, s):
+        """Lattice updates per second the session requests: cells x steps per frame x fps."""
+        return s.n * int(s.p.get('steps', self.steps_per_frame)) / self.period
 
     def _fail(self, s, err):
         """A session whose tunnel raised: reported, retired, its memory released; the others
@@ -346,6 +439,7 @@ class SessionServer:
         self._invalidate(s)
         self.active.pop(s.id, None)
         self.used -= s.bytes
+        self.demand -= getattr(s, 'demand', 0.0)
         try:
             s.solver.synchronize()
         except Exception:
@@ -364,14 +458,15 @@ class SessionServer:
         for s in gone:
             del self.active[s.id]
             self.used -= s.bytes
+            self.demand -= getattr(s, 'demand', 0.0)
             s.solver.synchronize()
             s.solver = None
             self.retired += 1
 
     # ---- one round ----
     def round(self):
-        """Retire, admit, then serve every session with an outstanding request. Returns the
-        number of frames produced."""
+        """Retire, admit, then serve every session with an outstanding request, oldest request
+        first, and collect the frames as they complete. Returns the number of frames produced."""
         now = self.clock()
         if self.t0 is None:
             self.t0 = now
@@ -380,12 +475,14 @@ class SessionServer:
         self._retire(now)
         self._admit(now)
         t_admit = self.clock()
-        due = [s for s in self.active.values() if self._due(s, now)]
+        due = sorted((s for s in self.active.values() if self._due(s, now)), key=lambda s: s.request_t)
+        self.max_active = max(self.max_active, len(self.active))
         if not due:
             self.phase['admit'] += t_admit - now
             return 0
         ks = {s.id: self._frame_steps(s) for s in due}
-        stepping = [s for s in due if ks[s.id] > 0]
+        # the batch holds its tunnels in id order, so the order of requests never rebuilds it
+        stepping = sorted((s for s in due if ks[s.id] > 0), key=lambda s: s.id)
         started = done = None
         if stepping:
             key = tuple(s.id for s in stepping)
@@ -411,50 +508,31 @@ class SessionServer:
             k = ks[s.id]
             try:
                 if k:
-                    s.solver.wait_event(done)
+                    # the streams executor stepped this tunnel on its own stream, which orders
+                    # its frame after its own steps; the persistent one steps all at once
+                    if self.batch_mode != 'streams':
+                        s.solver.wait_event(done)
                     s.solver.advance_particles(k, s.p)
                 s.frame_no += 1
                 s.solver.launch_frame_packed(s.p, self._want_cp(s))
             except Exception as e:
                 broken[s.id] = e
         t_issue = self.clock()
-        for s in due:
-            if s.id in broken:
+        pending = [s for s in due if s.id not in broken]
+        while pending:  # frames in the order they complete
+            ready = [s for s in pending if s.solver.frame_ready()]
+            if not ready:
+                time.sleep(20e-6)
                 continue
-            sv = s.solver
-            k = ks[s.id]
-            header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=sv.num_verts, forces=None, steps=k,
-                          mlups=s.mlups if (self.rate_in_header and s.running) else 0.0, running=s.running)
-            t_prev = s.last_t
-            try:
-                frame = sv.collect_frame_packed(header)
-            except Exception as e:
-                broken[s.id] = e
-                continue
-            t = self.clock()
-            self.latencies.append(t - s.request_t)
-            self.round_frames.append((s.id, frame))
-            if self.keep_frames:
-                self.frame_log.append((s.id, frame))
-            s.last_frame = frame
-            s.frames += 1
-            s.steps += k
-            s.last_t = t
-            self.cell_updates += s.n * k
-            fx, fy = float(sv.last_forces6[0]), float(sv.last_forces6[1])
-            q = 0.5 * s.p['uIn'] ** 2 * max(1, s.frontal)  # the client's Cd/Cl (web/js/main.js:337-339)
-            s.cd, s.cl = fx / q, fy / q
-            s.mlups = s.n * k / max(1e-9, t - t_prev) / 1e6
-            if self.pacing == 'client':
-                s.ready = False  # until the client acknowledges this frame
-            else:
-                # the client acknowledges at once and asks again at its next tick
-                s.request_t = max(t, s.request_t + (self.period if s.running else self.paused_period))
+            for s in ready:
+                pending.remove(s)
+                self._collect(s, ks[s.id], broken)
         for s in due:
             if s.id in broken:
                 self._fail(s, broken[s.id])
         t_end = self.clock()
         if started is not None:  # every frame has been collected, so both events are complete
+            done.synchronize()
             self.step_gpu_s += started.elapsed_time(done) / 1e3
             self.step_cells += sum(s.n * ks[s.id] for s in stepping if s.id not in broken)
         for name, a, b in (('admit', now, t_admit), ('rebuild', t_admit, t_rebuild), ('issue', t_rebuild, t_issue),
@@ -465,6 +543,37 @@ class SessionServer:
         self.active_sum += len(self.active)
         return len(due) - len(broken)
 
+    def _collect(self, s, k, broken):
+        """Take a session's finished frame: header, latency, the client's Cd/Cl and request."""
+        sv = s.solver
+        header = dict(type='frame', dims=list(s.dims), numP=sv.num_p, numVerts=sv.num_verts, forces=None, steps=k,
+                      mlups=s.mlups if (self.rate_in_header and s.running) else 0.0, running=s.running)
+        t_prev = s.last_t
+        try:
+            frame = sv.collect_frame_packed(header)
+        except Exception as e:
+            broken[s.id] = e
+            return
+        t = self.clock()
+        self.latencies.append(t - s.request_t)
+        self.round_frames.append((s.id, frame))
+        if self.keep_frames:
+            self.frame_log.append((s.id, frame))
+        s.last_frame = frame
+        s.frames += 1
+        s.steps += k
+        s.last_t = t
+        self.cell_updates += s.n * k
+        fx, fy = float(sv.last_forces6[0]), float(sv.last_forces6[1])
+        q = 0.5 * s.p['uIn'] ** 2 * max(1, s.frontal)  # the client's Cd/Cl (web/js/main.js:337-339)
+        s.cd, s.cl = fx / q, fy / q
+        s.mlups = s.n * k / max(1e-9, t - t_prev) / 1e6
+        if self.pacing == 'client':
+            s.ready = False  # until the client acknowledges this frame
+        else:
+            # the client acknowledges at once and asks again at its next tick
+            s.request_t = max(t, s.request_t + (self.period if s.running else self.paused_period))
+
     def stats(self):
         now = self.clock()
         lat = np.array(self.latencies) * 1e3 if self.latencies else np.zeros(1)
@@ -474,7 +583,7 @@ class SessionServer:
                 'p99_ms': round(float(np.percentile(lat, 99)), 2), 'max_ms': round(float(lat.max()), 2),
                 'rounds': self.rounds, 'batch_rebuilds': self.rebuilds, 'admitted': self.admitted,
                 'retired': self.retired, 'abandoned': self.abandoned, 'failed': self.failed,
-                'active_end': len(self.active),
+                'active_end': len(self.active), 'building_end': len(self.building),
                 'max_active': self.max_active,
                 'mean_active': round(self.active_sum / max(1, self.rounds), 1), 'queued_end': len(self.queue),
                 'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
@@ -484,7 +593,9 @@ class SessionServer:
                 'step_share_of_wall': round(self.step_gpu_s / span, 3),
                 'round_ms': {'p50': round(float(np.percentile(rs, 50)), 1), 'p99': round(float(np.percentile(rs, 99)), 1),
                              **{f'{k}_mean': round(v / max(1, self.rounds) * 1e3, 2) for k, v in self.phase.items()}},
-                'frames_per_session_s': round(len(self.latencies) / span / max(1e-9, self.active_sum / max(1, self.rounds)), 2)}
+                'frames_per_session_s': round(len(self.latencies) / span / max(1e-9, self.active_sum / max(1, self.rounds)), 2),
+                'requested_glups_end': round(self.demand / 1e9, 2),
+                'work_bound_glups': None if self.work_bound is None else round(self.work_bound / 1e9, 2)}
 
     def reset_window(self):
         """Start a fresh measurement window (drop latencies and counters so far)."""
@@ -498,6 +609,15 @@ class SessionServer:
         self.t0 = self.clock()
 
     def close(self):
+        if self._jobs is not None:  # stop the admission worker once it has finished its tunnel
+            self._jobs.put(None)
+            self._worker.join()
+            self._jobs = None
+            while self._built:
+                s, _ = self._built.popleft()
+                if s.solver is not None:
+                    s.solver.synchronize()
+            self.building.clear()
         if self._batch is not None:
             self._batch.close()
             self._batch, self._batch_key = None, None
@@ -553,7 +673,7 @@ class Arrivals:
 
 def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='fp32', seed=5, device='cuda:0',
              particles=5000, warm_start=True, tile=0, steps_per_frame=10, fps=30.0, mask_set=None, keep=None,
-             before_window=None, latencies_out=None, server_factory=None, warmup_s=0.0):
+             before_window=None, latencies_out=None, server_factory=None, warmup_s=0.0, work_bound_glups=None):
     """Config 5 in wall-clock time: Poisson arrivals at `rate` per second for `duration`
     seconds, each session requesting `fps` frames per second of its particles, one slice and
     Cd/Cl, admitted against `budget` bytes. With warm_start the run begins from the arrival
@@ -570,7 +690,8 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     SessionServer constructor (same arguments)."""
     gen = Arrivals(seed, mean_life, particles, mask_set)
     srv = (server_factory or SessionServer)(device, budget_bytes=budget, precision=precision, fps=fps,
-                                            steps_per_frame=steps_per_frame, tile=tile)
+                                            steps_per_frame=steps_per_frame, tile=tile, admit_thread=True,
+                                            work_bound_glups=work_bound_glups)
 
     def offer(s, t):
         if keep is None or keep(s, t):
@@ -581,6 +702,9 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
         for _ in range(int(gen.rng.poisson(rate * mean_life))):
             offer(gen.session(start), 0.0)
         srv._admit(start)
+        while srv.building:  # the worker builds the stationary sessions' tunnels
+            time.sleep(0.01)
+            srv._admit(time.perf_counter())
         srv.round()  # the stationary sessions have been running: one round builds their batch
         t_warm = time.perf_counter()
         while time.perf_counter() - t_warm < warmup_s:
