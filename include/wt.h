@@ -102,11 +102,12 @@ int wt_links_scan(const wt_grid* g, int64_t* scratch, int64_t* count_dev, void* 
 int wt_links_fill(const wt_grid* g, const int64_t* scratch, int32_t* cells, uint32_t* masks, int64_t capacity,
                   void* stream);
 
-/* Tile variants of the step kernel: writes up to `cap` rows of 4 ints into out and returns
- * the count. Direct-load tiles: {id, cells_per_thread, threads_per_block,
- * min_blocks_per_sm}; streaming tiles (shared-memory staging through bulk async copies):
- * {id, -chunk_cells, threads_per_block, pipeline_stages}. Select one with wt_grid.tile. */
-int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap);
+/* Tile variants of the step kernel for a storage precision and collision form (WT_COLLIDE_*):
+ * writes up to `cap` rows of 4 ints into out and returns the count. Direct-load and row-grid
+ * tiles: {id, cells_per_thread, threads_per_block, min_blocks_per_sm}; streaming tiles
+ * (shared-memory staging through bulk async copies): {id, -chunk_cells, threads_per_block,
+ * pipeline_stages}. Select one with wt_grid.tile. */
+int wt_step_tiles(int32_t precision, int32_t collision, int32_t* out, int32_t cap);
 
 /* ---- hot path ---- */
 /* `steps` launches of step_kernel (server/lbm.py:72-166), issued by Solver.step
@@ -114,7 +115,8 @@ int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap);
  * regularized collision with Smagorinsky eddy viscosity and the outlet sponge. Reads
  * f[cur], writes f[cur ^ 1], alternating; the final populations are in f[cur ^ (steps & 1)].
  * Face cells see exactly the neighbour values the reference's serial (Warp CPU) order
- * gives. Each step is two kernels. */
+ * gives. Each step is two kernels (three with the pipelined tiles, which split the bulk
+ * update between a kernel for plain interior cell pairs and one for the rest). */
 int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
             void* stream);
 /* Test entry point for the failure path; no counterpart in the reference. wt_step with chunk

@@ -50,7 +50,7 @@ def admissible(solver):
     cells per thread; streaming tiles (negative second field) need nx divisible by 16."""
     out = []
     elem = {W.F32: 4, W.F16: 2, W.BF16: 2, W.F64: 8}[solver.precision]
-    for t in W.step_tiles(solver.precision):
+    for t in W.step_tiles(solver.precision, solver.collision):
         v = t[1]
         if v > 0 and (solver.nx % v or (solver.precision == W.F64 and v == 4)):
             continue

@@ -122,7 +122,8 @@ static int launch_pipe(const void* args, int32_t n, cudaStream_t st) {
     {25, 2, 2, 128, 9, 0, 0, launch_rows<PREC, FAST, 128, 9, 0>},                        \
     {26, 2, 2, 128, 10, 0, 0, launch_rows<PREC, FAST, 128, 10, 0>}
 
-// pipelined row forms (kind 3, k_step_pipe, half-width storage only): two cells per thread,
+// pipelined row forms (kind 3, k_step_pipe, half-width storage and the moment-space collision
+// only): two cells per thread,
 // threads per block, resident blocks per SM, and in the last field the rows per block
 #define WT_VARIANTS_HALF(PREC, FAST)                                                     \
     {27, 3, 2, 128, 7, 0, 4, launch_pipe<PREC, FAST, 128, 7, 4>},                        \
@@ -132,7 +133,7 @@ static int launch_pipe(const void* args, int32_t n, cudaStream_t st) {
 
 template <int PREC, bool FAST>
 const StepVariant* variants_of(int* count) {
-    if constexpr (sizeof(typename Prec<PREC>::S) == 2) {
+    if constexpr (sizeof(typename Prec<PREC>::S) == 2 && FAST) {
         static const StepVariant table[] = {WT_VARIANTS(PREC, FAST), WT_VARIANTS_HALF(PREC, FAST)};
         *count = (int)(sizeof(table) / sizeof(table[0]));
         return table;

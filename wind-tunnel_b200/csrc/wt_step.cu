@@ -33,14 +33,17 @@ extern "C" int wt_step_test_skip_chunk(const wt_grid* g, int32_t cur, int32_t st
     return step_any(g, cur, steps, uin, tau, smag, flags, skip_chunk, stream);
 }
 
-extern "C" int wt_step_tiles(int32_t precision, int32_t* out, int32_t cap) {
+extern "C" int wt_step_tiles(int32_t precision, int32_t collision, int32_t* out, int32_t cap) {
+    if (collision != WT_COLLIDE_EXACT && collision != WT_COLLIDE_FAST)
+        return wt_set_error(WT_ERR_ARG, "wt_step_tiles: unknown collision form %d", collision);
+    const bool fast = collision == WT_COLLIDE_FAST;
     int count = 0;
     const wt::StepVariant* t = nullptr;
     switch (precision) {
-        case WT_F32: t = wt::step_variants<WT_F32>(false, &count); break;
-        case WT_F16: t = wt::step_variants<WT_F16>(false, &count); break;
-        case WT_BF16: t = wt::step_variants<WT_BF16>(false, &count); break;
-        case WT_F64: t = wt::step_variants<WT_F64>(false, &count); break;
+        case WT_F32: t = wt::step_variants<WT_F32>(fast, &count); break;
+        case WT_F16: t = wt::step_variants<WT_F16>(fast, &count); break;
+        case WT_BF16: t = wt::step_variants<WT_BF16>(fast, &count); break;
+        case WT_F64: t = wt::step_variants<WT_F64>(fast, &count); break;
         default: return wt_set_error(WT_ERR_ARG, "wt_step_tiles: unknown precision %d", precision);
     }
     for (int k = 0; k < count && k < cap; ++k) {

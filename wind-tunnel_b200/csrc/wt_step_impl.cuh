@@ -1223,96 +1223,130 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 
 constexpr int PIPE_WORDS = Q + 10;  // 19 aligned pairs, then the neighbour pairs of cx != 0
 
+// Address checks of the pipelined kernel, compiled in only with -DWT_PIPE_CHECK (a diagnostic
+// build): an access outside [lo, hi) or off its alignment is skipped and its site recorded in
+// the tunnel's status word (WT_ERR_ARG - 100 * site), so a bad index is reported, not used.
+#ifdef WT_PIPE_CHECK
+#define WT_PIPE_OK(site, p, lo, hi, al)                                                              \
+    ((reinterpret_cast<uintptr_t>(p) >= reinterpret_cast<uintptr_t>(lo) &&                            \
+      reinterpret_cast<uintptr_t>(p) + (al) <= reinterpret_cast<uintptr_t>(hi) &&                     \
+      reinterpret_cast<uintptr_t>(p) % (al) == 0) ||                                                  \
+     (a.status && (atomicExch(a.status, WT_ERR_ARG - 100 * (site)), true) && false))
+#else
+#define WT_PIPE_OK(site, p, lo, hi, al) true
+#endif
+
 template <int PREC, bool FAST, int BLOCK, int MINB, int ROWS>
 __global__ void __launch_bounds__(BLOCK, MINB)
-    k_step_pipe(const __grid_constant__ RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
+    k_step_pipe(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
     using P = Prec<PREC>;
     using S = typename P::S;
     using T = typename P::T;
     static_assert(sizeof(S) == 2, "the pipelined tile stages pairs of half-width values as 4-byte words");
+    static_assert(FAST, "the pipelined tile runs the moment-space collision (no shift table in its loop)");
     __shared__ uint32_t stage[2][PIPE_WORDS][BLOCK];
     __shared__ uint32_t stage_code[2][BLOCK];
-    const auto& a = r.a;
+    const StepArgs<S, T>& a = r.a;
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
     const int32_t tid = (int32_t)threadIdx.x;
     const int32_t xruns = (nx / 2 + BLOCK - 1) / BLOCK;
     const int32_t row0 = (int32_t)blockIdx.x * ROWS;
     const int32_t items = min(ROWS, ny * nz - row0) * xruns;
-    // item j: row row0 + j / xruns, pair x0 = 2 (BLOCK (j % xruns) + tid)
-    auto place = [&](int32_t j, int32_t& row, int32_t& x0, int32_t& y, int32_t& z) {
-        const int32_t rr = j / xruns;
-        row = row0 + rr;
-        x0 = ((j - rr * xruns) * BLOCK + tid) * 2;
-        z = (int32_t)a.dny.div((uint32_t)row);
-        y = row - z * ny;
-    };
-    auto issue = [&](int32_t j) {  // stage item j's pull into buffer j & 1 (pairs that may be pure)
-        if (j >= items) return;
-        int32_t row, x0, y, z;
-        place(j, row, x0, y, z);
-        if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1 || x0 == 0 || x0 + 2 >= nx) return;
-        const int32_t idx0 = x0 + row * nx;
-        const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * 2;
-        const int b = j & 1;
-        int k = Q;
-        // offsets read afresh for every item (a volatile read of the grid constant)
-        const volatile int64_t* loff = r.loff;
-        unroll<0, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            const char* w = fb + loff[i];  // the aligned pair (x0, x0 + 1) of the source row
-            cp_async4(&stage[b][i][tid], w);
-            // the pair holding x0 - 1 (cx > 0) or x0 + 2 (cx < 0), inside the source row
-            // (0 < x0 < nx - 2)
-            if constexpr (cx(i) > 0) cp_async4(&stage[b][k++][tid], w - 4);
-            if constexpr (cx(i) < 0) cp_async4(&stage[b][k++][tid], w + 4);
-        });
-        cp_async4(&stage_code[b][tid], a.code + (idx0 & ~3));
-    };
-    issue(0);
-    cp_async_commit();
-#pragma unroll 1
-    for (int32_t j = 0; j < items; ++j) {
-        issue(j + 1);
+#ifdef WT_PIPE_CHECK
+    const char* f_lo = reinterpret_cast<const char*>(a.fin);
+    const char* f_hi = f_lo + (int64_t)Q * a.n * 2;
+    const char* c_hi = reinterpret_cast<const char*>(a.code) + a.n;
+    char* o_lo = reinterpret_cast<char*>(a.dst[0]);
+    char* o_hi = o_lo + (int64_t)Q * a.n * 2;
+#endif
+    // prologue: stage item 0 (items run j = row * xruns + xrun; pair x0 = 2 (BLOCK xrun + tid))
+    for (int32_t j = 0; j <= items; ++j) {
+        // ---- stage item j + 1 (j = -1 .. items - 1 in effect: the loop runs one ahead) ----
+        const int32_t jn = j;  // the item staged in this pass
+        if (jn < items) {
+            const int32_t rr = jn / xruns;
+            const int32_t row = row0 + rr;
+            const int32_t x0 = ((jn - rr * xruns) * BLOCK + tid) * 2;
+            const int32_t z = (int32_t)a.dny.div((uint32_t)row);
+            const int32_t y = row - z * ny;
+            if (!(y == 0 || y == ny - 1 || z == 0 || z == nz - 1 || x0 == 0 || x0 + 2 >= nx)) {
+                const int32_t idx0 = x0 + row * nx;
+                const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * 2;
+                const int b = jn & 1;
+                int k = Q;
+#pragma unroll
+                for (int i = 0; i < Q; ++i) {
+                    const char* w = fb + r.loff[i];  // the aligned pair (x0, x0 + 1) of the source row
+                    if (WT_PIPE_OK(1, w, f_lo, f_hi, 4)) cp_async4(&stage[b][i][tid], w);
+                    // the pair holding x0 - 1 (cx > 0) or x0 + 2 (cx < 0), inside the source row
+                    if (cx(i) > 0) {
+                        if (WT_PIPE_OK(2, w - 4, f_lo, f_hi, 4)) cp_async4(&stage[b][k][tid], w - 4);
+                        ++k;
+                    }
+                    if (cx(i) < 0) {
+                        if (WT_PIPE_OK(3, w + 4, f_lo, f_hi, 4)) cp_async4(&stage[b][k][tid], w + 4);
+                        ++k;
+                    }
+                }
+                const uint8_t* cw = a.code + (idx0 & ~3);
+                if (WT_PIPE_OK(4, cw, a.code, c_hi, 4)) cp_async4(&stage_code[b][tid], cw);
+            }
+        }
         cp_async_commit();
-        cp_async_wait1();  // this thread's copies of item j have landed
-        int32_t row, x0, y, z;
-        place(j, row, x0, y, z);
+        if (j == 0) continue;
+        cp_async_wait1();  // this thread's copies of item j - 1 have landed
+        // ---- compute item jc = j - 1 from its stage ----
+        const int32_t jc = j - 1;
+        const int32_t rr = jc / xruns;
+        const int32_t row = row0 + rr;
+        const int32_t x0 = ((jc - rr * xruns) * BLOCK + tid) * 2;
+        const int32_t z = (int32_t)a.dny.div((uint32_t)row);
+        const int32_t y = row - z * ny;
         const bool interior_row = !(y == 0 || y == ny - 1 || z == 0 || z == nz - 1);
         const bool staged = interior_row && x0 > 0 && x0 + 2 < nx;
-        const int b = j & 1;
+        const int b = jc & 1;
         const int32_t idx0 = x0 + row * nx;
         const uint32_t codes = staged ? (stage_code[b][tid] >> (8 * (idx0 & 3))) & 0xffffu : 0xffffu;
         if (!pure_pair(interior_row, staged, codes, x0, nx)) continue;  // left to k_step_rows
         T f[2][Q];
         int k = Q;
-        unroll<0, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
             S v[2], e[2];
             const uint32_t w = stage[b][i][tid];
             memcpy(v, &w, 4);
-            if constexpr (cx(i) == 0) {
-                f[0][i] = ld_in<P, FAST, i>(a, &v[0]);
-                f[1][i] = ld_in<P, FAST, i>(a, &v[1]);
+            if (cx(i) == 0) {
+                f[0][i] = P::to(v[0]);
+                f[1][i] = P::to(v[1]);
             } else {
-                const uint32_t wn = stage[b][k++][tid];
+                const uint32_t wn = stage[b][k][tid];
+                ++k;
                 memcpy(e, &wn, 4);
-                if constexpr (cx(i) > 0) {
-                    f[0][i] = ld_in<P, FAST, i>(a, &e[1]);  // x0 - 1
-                    f[1][i] = ld_in<P, FAST, i>(a, &v[0]);
+                if (cx(i) > 0) {
+                    f[0][i] = P::to(e[1]);  // x0 - 1
+                    f[1][i] = P::to(v[0]);
                 } else {
-                    f[0][i] = ld_in<P, FAST, i>(a, &v[1]);
-                    f[1][i] = ld_in<P, FAST, i>(a, &e[0]);  // x0 + 2
+                    f[0][i] = P::to(v[1]);
+                    f[1][i] = P::to(e[0]);  // x0 + 2
                 }
             }
-        });
+        }
         T m[2][4];
         collide_two<P, FAST>(a, f, x0, m);
-        char* ob = reinterpret_cast<char*>(a.dst[0]) + (int64_t)idx0 * (int64_t)sizeof(S);
-        const volatile int64_t* soff = r.soff;
-        unroll<0, Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            store_cells<P, FAST, 2, i>(a, reinterpret_cast<S*>(ob + soff[i]), f);
-        });
+        char* ob = reinterpret_cast<char*>(a.dst[0]) + (int64_t)idx0 * 2;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            uint32_t w;
+            if constexpr (std::is_same<S, __half>::value) {
+                const __half2 h = __floats2half2_rn(f[0][i], f[1][i]);
+                memcpy(&w, &h, 4);
+            } else {
+                const __nv_bfloat162 h = __floats2bfloat162_rn(f[0][i], f[1][i]);
+                memcpy(&w, &h, 4);
+            }
+            char* o = ob + r.soff[i];
+            if (WT_PIPE_OK(5, o, o_lo, o_hi, 4)) *reinterpret_cast<uint32_t*>(o) = w;
+        }
         // mac where faces read it: a pure pair holds neither x = 1 nor x = nx - 2
         if (a.mac_all || y == 1 || y == ny - 2 || z == 1 || z == nz - 2) {
             store_mac(a.mac_cur, idx0, m[0][0], m[0][1], m[0][2], m[0][3]);

@@ -67,7 +67,7 @@ def lib():
             'wt_links_scratch_len': ([i64], i64),
             'wt_links_scan': ([gp, vp, vp, vp], ctypes.c_int),
             'wt_links_fill': ([gp, vp, vp, vp, i64, vp], ctypes.c_int),
-            'wt_step_tiles': ([i32, vp, i32], ctypes.c_int),
+            'wt_step_tiles': ([i32, i32, vp, i32], ctypes.c_int),
             'wt_step': ([gp, i32, i32, f64, f64, f64, i32, vp], ctypes.c_int),
             'wt_step_test_skip_chunk': ([gp, i32, i32, f64, f64, f64, i32, i32, vp], ctypes.c_int),
             'wt_reduce_scratch_len': ([i64], i64),
@@ -114,10 +114,13 @@ def ptr(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
-def step_tiles(precision):
-    """[(id, cells_per_thread, threads_per_block, min_blocks_per_sm), ...] of the step kernel."""
+def step_tiles(precision, collision=COLLIDE_EXACT):
+    """[(id, cells_per_thread, threads_per_block, min_blocks_per_sm), ...] of the step kernel for
+    a storage precision and collision form (COLLIDE_EXACT / COLLIDE_FAST, or 'exact' / 'fast')."""
+    if isinstance(collision, str):
+        collision = {'exact': COLLIDE_EXACT, 'fast': COLLIDE_FAST}[collision]
     buf = (ctypes.c_int32 * 256)()
-    n = lib().wt_step_tiles(int(precision), buf, 64)
+    n = lib().wt_step_tiles(int(precision), int(collision), buf, 64)
     if n < 0:
         check(n)
     return [tuple(buf[4 * k:4 * k + 4]) for k in range(n)]
