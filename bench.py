@@ -246,7 +246,8 @@ def run_ours(args, rank, world, local_rank):
     hbm, peak_kind = peaks()
     achieved = ALGO_BYTES[prec] * n / t_step / 1e9
     copy_here = copy_bandwidth(dev)
-    traffic = profile_traffic(f'step_{prec}_{nx}x{ny}x{nz}.md')
+    # DRAM bytes per step from the committed capture (a 384x192x192 case scaled to the full grid)
+    traffic = profile_traffic(f'step_{prec}_384x192x192.md') if (nx, ny, nz) == (512, 256, 256) else None
     roofline = {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': hbm, 'unit': 'GB/s',
                 'frac': round(achieved / hbm, 4), 'traffic': traffic,
                 'peak_source': f'{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)' if peak_kind == 'measured'

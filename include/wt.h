@@ -115,8 +115,7 @@ int wt_step_tiles(int32_t precision, int32_t collision, int32_t* out, int32_t ca
  * regularized collision with Smagorinsky eddy viscosity and the outlet sponge. Reads
  * f[cur], writes f[cur ^ 1], alternating; the final populations are in f[cur ^ (steps & 1)].
  * Face cells see exactly the neighbour values the reference's serial (Warp CPU) order
- * gives. Each step is two kernels (three with the pipelined tiles, which split the bulk
- * update between a kernel for plain interior cell pairs and one for the rest). */
+ * gives. Each step is two kernels (one with the fused-face row tiles). */
 int wt_step(const wt_grid* g, int32_t cur, int32_t steps, double uin, double tau, double smag, int32_t flags,
             void* stream);
 /* Test entry point for the failure path; no counterpart in the reference. wt_step with chunk

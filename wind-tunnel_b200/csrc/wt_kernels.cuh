@@ -40,7 +40,7 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     return WT_OK;
 }
 
-template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR>
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false>
 static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     using P = Prec<PREC>;
     using S = typename P::S;
@@ -56,35 +56,7 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
         r.soff[i] = (int64_t)i * a.n * (int64_t)sizeof(S);
     }
     const dim3 grid((unsigned)((a.nx / 2 + BLOCK - 1) / BLOCK), (unsigned)a.ny, (unsigned)a.nz);
-    k_step_rows<PREC, FAST, BLOCK, MINB, ADDR><<<grid, BLOCK, 0, st>>>(r);
-    return WT_OK;
-}
-
-template <int PREC, bool FAST, int BLOCK, int MINB, int ROWS>
-static int launch_pipe(const void* args, int32_t n, cudaStream_t st) {
-    using P = Prec<PREC>;
-    using S = typename P::S;
-    using T = typename P::T;
-    (void)n;
-    RowArgs<S, T> r;
-    r.a = *static_cast<const StepArgs<S, T>*>(args);
-    const StepArgs<S, T>& a = r.a;
-    for (int i = 0; i < Q; ++i) {
-        r.loff[i] = ((int64_t)i * a.n - (int64_t)cy(i) * a.nx - (int64_t)cz(i) * a.nxy) * (int64_t)sizeof(S);
-        r.soff[i] = (int64_t)i * a.n * (int64_t)sizeof(S);
-    }
-    static bool configured = false;
-    if (!configured) {  // MINB blocks of double-buffered stages need most of the SM's shared memory
-        if (cudaFuncSetAttribute(k_step_pipe<PREC, FAST, BLOCK, MINB, ROWS>,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
-            return wt_cuda_check("wt_step: shared-memory carve-out");
-        configured = true;
-    }
-    const int32_t nrows = a.ny * a.nz;
-    k_step_pipe<PREC, FAST, BLOCK, MINB, ROWS><<<(unsigned)((nrows + ROWS - 1) / ROWS), BLOCK, 0, st>>>(r);
-    // then every pair the pipelined kernel leaves (tile 19's shape)
-    const dim3 grid((unsigned)((a.nx / 2 + 127) / 128), (unsigned)a.ny, (unsigned)a.nz);
-    k_step_rows<PREC, FAST, 128, 8, 0, true><<<grid, 128, 0, st>>>(r);
+    k_step_rows<PREC, FAST, BLOCK, MINB, ADDR, FUSE><<<grid, BLOCK, 0, st>>>(r);
     return WT_OK;
 }
 
@@ -92,7 +64,9 @@ static int launch_pipe(const void* args, int32_t n, cudaStream_t st) {
 // resident blocks per SM. Streaming forms (kind 1): chunk length L, pipeline stages NS,
 // threads per block, blocks per SM. Row-grid forms (kind 2, k_step_rows): two cells per
 // thread, threads per block, minimum resident blocks per SM, and in the last field the
-// addressing form (0: per-population bases, 1: one base plus byte offsets). wt_grid.tile
+// addressing form (0: per-population bases, 1: one base plus byte offsets); kind 4 is the row
+// grid with the face cells of k_step_faces computed by the blocks of the rows they read
+// (k_step_rows with FUSE), so the step is one kernel. wt_grid.tile
 // selects one (0 = the default for the precision and collision form); autotune.py times them.
 #define WT_VARIANTS(PREC, FAST)                                                          \
     {1, 0, 1, 256, 4, 0, 0, launch_bulk<PREC, FAST, 1, 256, 4>},                         \
@@ -120,28 +94,15 @@ static int launch_pipe(const void* args, int32_t n, cudaStream_t st) {
     {23, 2, 2, 256, 4, 0, 1, launch_rows<PREC, FAST, 256, 4, 1>},                        \
     {24, 2, 2, 128, 4, 0, 0, launch_rows<PREC, FAST, 128, 4, 0>},                        \
     {25, 2, 2, 128, 9, 0, 0, launch_rows<PREC, FAST, 128, 9, 0>},                        \
-    {26, 2, 2, 128, 10, 0, 0, launch_rows<PREC, FAST, 128, 10, 0>}
-
-// pipelined row forms (kind 3, k_step_pipe, half-width storage and the moment-space collision
-// only): two cells per thread,
-// threads per block, resident blocks per SM, and in the last field the rows per block
-#define WT_VARIANTS_HALF(PREC, FAST)                                                     \
-    {27, 3, 2, 128, 7, 0, 4, launch_pipe<PREC, FAST, 128, 7, 4>},                        \
-    {28, 3, 2, 128, 7, 0, 8, launch_pipe<PREC, FAST, 128, 7, 8>},                        \
-    {29, 3, 2, 64, 14, 0, 4, launch_pipe<PREC, FAST, 64, 14, 4>},                        \
-    {30, 3, 2, 128, 7, 0, 16, launch_pipe<PREC, FAST, 128, 7, 16>}
+    {26, 2, 2, 128, 10, 0, 0, launch_rows<PREC, FAST, 128, 10, 0>},                      \
+    {27, 4, 2, 128, 8, 0, 0, launch_rows<PREC, FAST, 128, 8, 0, true>},                  \
+    {28, 4, 2, 64, 16, 0, 0, launch_rows<PREC, FAST, 64, 16, 0, true>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants_of(int* count) {
-    if constexpr (sizeof(typename Prec<PREC>::S) == 2 && FAST) {
-        static const StepVariant table[] = {WT_VARIANTS(PREC, FAST), WT_VARIANTS_HALF(PREC, FAST)};
-        *count = (int)(sizeof(table) / sizeof(table[0]));
-        return table;
-    } else {
-        static const StepVariant table[] = {WT_VARIANTS(PREC, FAST)};
-        *count = (int)(sizeof(table) / sizeof(table[0]));
-        return table;
-    }
+    static const StepVariant table[] = {WT_VARIANTS(PREC, FAST)};
+    *count = (int)(sizeof(table) / sizeof(table[0]));
+    return table;
 }
 
 template <int PREC>
@@ -149,14 +110,18 @@ const StepVariant* step_variants(bool fast, int* count) {
     return fast ? variants_of<PREC, true>(count) : variants_of<PREC, false>(count);
 }
 
-// defaults until the autotuner has measured the tunnel: two cells per thread at 64
-// registers (the fastest shape at 33.5M cells in fp32, fp16 and bf16); fp64 needs 128
-// registers to avoid spills, so it keeps two cells per thread at 128 registers
+// defaults until the autotuner has measured the tunnel (the fastest shapes at 33.5M cells):
+// two cells per thread at 64 registers, as the one-dimensional tile 18 for fp32 and the
+// reference-order collision, as the row-grid tile 21 (64 threads, 16 blocks per SM) for fp16 /
+// bf16 storage with the moment-space collision; fp64 needs 128 registers to avoid spills, so
+// it keeps two cells per thread at 128 registers (tile 4)
 template <int PREC>
 const StepVariant* pick_variant(const wt_grid* g) {
     int count;
-    const StepVariant* t = step_variants<PREC>(g->collision == WT_COLLIDE_FAST, &count);
-    const int want = g->tile > 0 ? g->tile : (PREC == WT_F64 ? 4 : 18);
+    const bool fast = g->collision == WT_COLLIDE_FAST;
+    const StepVariant* t = step_variants<PREC>(fast, &count);
+    const int dflt = PREC == WT_F64 ? 4 : ((PREC == WT_F16 || PREC == WT_BF16) && fast ? 21 : 18);
+    const int want = g->tile > 0 ? g->tile : dflt;
     for (int k = 0; k < count; ++k) {
         if (t[k].id != want) continue;
         if (g->nx % t[k].v != 0) return nullptr;
@@ -214,7 +179,7 @@ int step_prec(const wt_grid* g, int32_t cur, int32_t steps, double uin, double t
         a.mac_cur = static_cast<T*>(g->mac[cur ^ 1]);
         a.mac_all = (flags & WT_STEP_MAC_ALL_LAST) && s == steps - 1;
         if (int rc = var->launch(&a, a.n, stream)) return rc;
-        k_step_faces<PREC><<<nb_face, 256, 0, stream>>>(a);
+        if (var->kind != 4) k_step_faces<PREC><<<nb_face, 256, 0, stream>>>(a);
         cur ^= 1;
     }
     return wt_cuda_check("wt_step launch");

@@ -408,7 +408,9 @@ __device__ __forceinline__ F2 xcoord<F2>(int32_t x) { return F2((float)x, (float
 // lane at a time: its product-then-difference, compiled as paired operations, is fused by the
 // assembler into one paired FMA (paired multiplies feeding paired adds are fused whatever the
 // rounding modifiers and -fmad=false say), which rounds differently from the one-cell form;
-// per-lane evaluation keeps identical bits at a cost of a few instructions.
+// per-lane evaluation keeps identical bits at a cost of a few instructions. (Restating B with
+// every product feeding an FMA multiplicand, k45 tr(N) times -1/3, was tried: the pair form
+// still came out a last bit different from the one-cell form in some cells.)
 // With SHIFT the outputs are deviations from the shift e_i, so B also carries + 1.5 U^2.
 template <class T, bool SHIFT>
 struct BTerm {
@@ -859,10 +861,18 @@ __device__ __forceinline__ void pair_walls(const StepArgs<typename Prec<PREC>::S
     });
 }
 
+// the macro values (ux, uy, uz, rho) of a solid cell
+template <class T>
+__device__ __forceinline__ void solid_macro(T (&m)[4]) {
+    m[0] = (T)0.0; m[1] = (T)0.0; m[2] = (T)0.0; m[3] = (T)1.0;
+}
+
+// pair_finish hands the pair's macro values (what it writes to mac) back in mo.
 template <int PREC, bool FAST>
 __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                             int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
-                                            bool row_shell, typename Prec<PREC>::T (&f)[2][Q]) {
+                                            bool row_shell, typename Prec<PREC>::T (&f)[2][Q],
+                                            typename Prec<PREC>::T (&mo)[2][4]) {
     using P = Prec<PREC>;
     using T = typename P::T;
     const int32_t nx = a.nx;
@@ -874,6 +884,8 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
     if (sol0 && sol1) {
         if (wsol0) store_mac(a.mac_cur, idx0, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
         if (wsol1) store_mac(a.mac_cur, idx0 + 1, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
+        solid_macro(mo[0]);
+        solid_macro(mo[1]);
         return;
     }
     if ((c0 | c1) & CODE_NEAR) pair_walls<PREC, FAST>(a, idx0, c0, c1, f);
@@ -917,13 +929,22 @@ __device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::
             if (sol) store_mac(a.mac_cur, idx0 + k, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
             else store_mac(a.mac_cur, idx0 + k, m[k][0], m[k][1], m[k][2], m[k][3]);
         }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) mo[k][c] = sol ? (c == 3 ? (T)1.0 : (T)0.0) : m[k][c];
     }
+}
+template <int PREC, bool FAST>
+__device__ __forceinline__ void pair_finish(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                            int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
+                                            bool row_shell, typename Prec<PREC>::T (&f)[2][Q]) {
+    typename Prec<PREC>::T mo[2][4];
+    pair_finish<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, f, mo);
 }
 
 template <int PREC, bool FAST>
 __device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                               int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
-                                              bool row_shell) {
+                                              bool row_shell, typename Prec<PREC>::T (&mo)[2][4]) {
     using P = Prec<PREC>;
     using T = typename P::T;
     const bool sol0 = (codes & CODE_SOLID) != 0, sol1 = ((codes >> 8) & CODE_SOLID) != 0;
@@ -933,7 +954,14 @@ __device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>
         pair_load<PREC>(a, idx0, r);
         pair_unpack<P, FAST>(a, r, f);
     }
-    pair_finish<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, f);
+    pair_finish<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, f, mo);
+}
+template <int PREC, bool FAST>
+__device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                              int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
+                                              bool row_shell) {
+    typename Prec<PREC>::T mo[2][4];
+    interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, mo);
 }
 
 template <int PREC, bool FAST, int V>
@@ -1087,12 +1115,13 @@ struct RowArgs {
 template <int PREC, bool FAST>
 __device__ __forceinline__ void pair_lean_finish(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
                                                  typename Prec<PREC>::T (&f)[2][Q], int32_t idx0, int32_t x0,
-                                                 int32_t y, int32_t z, uint32_t codes, bool row_shell, bool offs);
+                                                 int32_t y, int32_t z, uint32_t codes, bool row_shell, bool offs,
+                                                 typename Prec<PREC>::T (&mo)[2][4]);
 
 template <int PREC, bool FAST, int ADDR>
 __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
                                           int32_t idx0, int32_t x0, int32_t y, int32_t z, uint32_t codes,
-                                          bool row_shell) {
+                                          bool row_shell, typename Prec<PREC>::T (&mo)[2][4]) {
     using P = Prec<PREC>;
     using S = typename P::S;
     using T = typename P::T;
@@ -1118,14 +1147,15 @@ __device__ __forceinline__ void pair_lean(const RowArgs<typename Prec<PREC>::S, 
             f[1][i] = ld_in<P, FAST, i>(a, p + 2);
         }
     });
-    pair_lean_finish<PREC, FAST>(r, f, idx0, x0, y, z, codes, row_shell, ADDR == 1);
+    pair_lean_finish<PREC, FAST>(r, f, idx0, x0, y, z, codes, row_shell, ADDR == 1, mo);
 }
 
 // The lean path after the pull: walls, collision, inlet / outlet, stores and mac (see k_step_rows).
 template <int PREC, bool FAST>
 __device__ __forceinline__ void pair_lean_finish(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
                                                  typename Prec<PREC>::T (&f)[2][Q], int32_t idx0, int32_t x0,
-                                                 int32_t y, int32_t z, uint32_t codes, bool row_shell, bool offs) {
+                                                 int32_t y, int32_t z, uint32_t codes, bool row_shell, bool offs,
+                                                 typename Prec<PREC>::T (&mo)[2][4]) {
     using P = Prec<PREC>;
     using S = typename P::S;
     using T = typename P::T;
@@ -1155,202 +1185,92 @@ __device__ __forceinline__ void pair_lean_finish(const RowArgs<typename Prec<PRE
     const bool w1 = a.mac_all || (!outlet && (row_shell || inlet));
     if (w0) store_mac(a.mac_cur, idx0, m[0][0], m[0][1], m[0][2], m[0][3]);
     if (w1) store_mac(a.mac_cur, idx0 + 1, m[1][0], m[1][1], m[1][2], m[1][3]);
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) mo[k][c] = m[k][c];
 }
 
-// the pure-pair test both kernels apply (codes: the pair's two code bytes)
-__device__ __forceinline__ bool pure_pair(bool interior_row, bool valid, uint32_t codes, int32_t x0, int32_t nx) {
-    return interior_row && valid && codes == 0 && x0 > 0 && x0 + 2 < nx;
+// The face cells that read this step's mac (k_step_faces: the y = ny-1 rows of interior z and the
+// z = nz-1 plane, x > 0) take it from one interior row each: a face cell at (x, y, z) reads the
+// cell (clamp(x), clamp(y), clamp(z)) clamped to the interior, and for these rows that is the row
+// (ny-2, z), (y, nz-2), (1, nz-2) or (ny-2, nz-2). With FUSE, the block of that interior row
+// computes them from its pair's own macro values right after the pair, so no separate kernel
+// (nor its launch and tail) is needed; the arithmetic is face_cell's, so the bits are too.
+// Face row (fy, fz), pair x0 (both cells of the row x0, x0 + 1), from the interior pair's values m.
+template <int PREC, bool FAST>
+__device__ __forceinline__ void fused_face_pair(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                                int32_t x0, int32_t fy, int32_t fz,
+                                                const typename Prec<PREC>::T (&m)[2][4]) {
+    using P = Prec<PREC>;
+    using T = typename P::T;
+    const int32_t nx = a.nx;
+    const int32_t fidx = x0 + nx * (fy + a.ny * fz);
+    const uint32_t codes = *reinterpret_cast<const uint16_t*>(a.code + fidx);
+    T fv[2][Q], fm[2][4];
+    bool fluid[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int32_t x = x0 + k;
+        const int j = x <= nx - 2 ? k : 0;  // clamp(x) to nx - 2: the pair's cell x0 (x = nx - 1)
+        fluid[k] = x > 0 && ((codes >> (8 * k)) & CODE_SOLID) == 0;  // x = 0: the face row's own block
+        face_values<T>(x, fy, fz, nx, a.ny, a.nz, a.uin, m[j][0], m[j][1], m[j][2], m[j][3], fm[k][3], fm[k][0],
+                       fm[k][1], fm[k][2]);
+        if (fluid[k]) eq_values<P, FAST>(a, fm[k][3], fm[k][0], fm[k][1], fm[k][2], fv[k]);
+    }
+    typename P::S* ob = a.dst[0] + fidx;
+    if (fluid[0] && fluid[1]) {
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            store_cells<P, FAST, 2, i>(a, ob + (int64_t)i * a.n, fv);
+        });
+    } else if (fluid[0] || fluid[1]) {
+        const int32_t k = fluid[0] ? 0 : 1;
+        unroll<0, Q>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            st_out<P, FAST, i>(a, ob + (int64_t)i * a.n + k, fluid[0] ? fv[0][i] : fv[1][i]);
+        });
+    }
+    if (a.mac_all) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (x0 + k == 0) continue;
+            if (fluid[k]) store_mac(a.mac_cur, fidx + k, fm[k][0], fm[k][1], fm[k][2], fm[k][3]);
+            else store_mac(a.mac_cur, fidx + k, (T)0.0, (T)0.0, (T)0.0, (T)1.0);
+        }
+    }
 }
 
-template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool SKIP_PURE = false>
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
+    using T = typename Prec<PREC>::T;
     const auto& a = r.a;
     const int32_t y = (int32_t)blockIdx.y, z = (int32_t)blockIdx.z;
-    const int32_t nx = a.nx;
+    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
     const int32_t x0 = ((int32_t)blockIdx.x * BLOCK + (int32_t)threadIdx.x) * 2;
     const bool valid = x0 < nx;
-    const int32_t idx0 = x0 + nx * (y + a.ny * z);
-    if (y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1) {  // a face row (uniform over the block)
+    const int32_t idx0 = x0 + nx * (y + ny * z);
+    if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {  // a face row (uniform over the block)
         bulk_cells<PREC, FAST, 2>(a, idx0, valid);
         return;
     }
-    const bool row_shell = y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2;
+    const bool row_shell = y == 1 || y == ny - 2 || z == 1 || z == nz - 2;
     const uint32_t codes = valid ? *reinterpret_cast<const uint16_t*>(a.code + idx0) : 0xffffu;
-    if constexpr (SKIP_PURE) {  // k_step_pipe has computed the pure pairs
-        const bool todo = valid && !pure_pair(true, valid, codes, x0, nx);
-        if (!__any_sync(0xffffffffu, todo)) return;
-        if (__all_sync(0xffffffffu, !todo || (codes & (CODE_SOLID * 0x0101u)) == 0)) {
-            if (todo) pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell);
-        } else if (todo) {
-            interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell);
-        }
-        return;
-    }
+    T m[2][4];
     // lean unless a cell of the warp is solid (or past the row's end)
     if (__all_sync(0xffffffffu, (codes & (CODE_SOLID * 0x0101u)) == 0)) {
-        pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell);
+        pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell, m);
     } else if (valid) {
-        interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell);
+        interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, m);
     }
-}
-
-// ---------------------------------------------------------------------------------
-// Pipelined row form for half-width storage (fp16 / bf16). The row kernel above waits on its
-// loads with one pair per thread in flight (64 registers hold one pair), so the step is bound
-// by load latency, not by HBM or issue. Here the work of a step is split in two kernels:
-//
-// * k_step_pipe computes every PURE pair: both cells plain interior fluid (code 0) in an
-//   interior row, neither the inlet nor the outlet pair. Each block walks ROWS lattice rows
-//   (items: the rows' x-runs of 2 * BLOCK cells) and every thread stages the pull of its NEXT
-//   item into shared memory with per-thread asynchronous copies (cp.async, 4 bytes each: the
-//   19 aligned pairs, the 10 pairs holding the x-shifted neighbours, the code word) while it
-//   computes the current one from the previous stage. The stage is double-buffered and each
-//   thread reads only the words it copied itself, so no block barrier is needed: the copies of
-//   item j + 1 go to the buffer of item j - 1, whose words this thread consumed in iteration
-//   j - 1. Its loop body is the pure path alone, which keeps every kernel parameter it does not
-//   need out of registers (a loop over the general paths spills).
-// * k_step_rows with SKIP_PURE then computes the rest (face rows, the inlet and outlet pairs,
-//   pairs next to walls or holding a solid cell) and leaves the pure pairs alone. Both decide
-//   purity by the same per-pair test, so every cell is written exactly once, by the same
-//   arithmetic as the other two-cell tiles: the results are bit for bit theirs.
-// ---------------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-constexpr int PIPE_WORDS = Q + 10;  // 19 aligned pairs, then the neighbour pairs of cx != 0
-
-// Address checks of the pipelined kernel, compiled in only with -DWT_PIPE_CHECK (a diagnostic
-// build): an access outside [lo, hi) or off its alignment is skipped and its site recorded in
-// the tunnel's status word (WT_ERR_ARG - 100 * site), so a bad index is reported, not used.
-#ifdef WT_PIPE_CHECK
-#define WT_PIPE_OK(site, p, lo, hi, al)                                                              \
-    ((reinterpret_cast<uintptr_t>(p) >= reinterpret_cast<uintptr_t>(lo) &&                            \
-      reinterpret_cast<uintptr_t>(p) + (al) <= reinterpret_cast<uintptr_t>(hi) &&                     \
-      reinterpret_cast<uintptr_t>(p) % (al) == 0) ||                                                  \
-     (a.status && (atomicExch(a.status, WT_ERR_ARG - 100 * (site)), true) && false))
-#else
-#define WT_PIPE_OK(site, p, lo, hi, al) true
-#endif
-
-template <int PREC, bool FAST, int BLOCK, int MINB, int ROWS>
-__global__ void __launch_bounds__(BLOCK, MINB)
-    k_step_pipe(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
-    using P = Prec<PREC>;
-    using S = typename P::S;
-    using T = typename P::T;
-    static_assert(sizeof(S) == 2, "the pipelined tile stages pairs of half-width values as 4-byte words");
-    static_assert(FAST, "the pipelined tile runs the moment-space collision (no shift table in its loop)");
-    __shared__ uint32_t stage[2][PIPE_WORDS][BLOCK];
-    __shared__ uint32_t stage_code[2][BLOCK];
-    const StepArgs<S, T>& a = r.a;
-    const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t tid = (int32_t)threadIdx.x;
-    const int32_t xruns = (nx / 2 + BLOCK - 1) / BLOCK;
-    const int32_t row0 = (int32_t)blockIdx.x * ROWS;
-    const int32_t items = min(ROWS, ny * nz - row0) * xruns;
-#ifdef WT_PIPE_CHECK
-    const char* f_lo = reinterpret_cast<const char*>(a.fin);
-    const char* f_hi = f_lo + (int64_t)Q * a.n * 2;
-    const char* c_hi = reinterpret_cast<const char*>(a.code) + a.n;
-    char* o_lo = reinterpret_cast<char*>(a.dst[0]);
-    char* o_hi = o_lo + (int64_t)Q * a.n * 2;
-#endif
-    // prologue: stage item 0 (items run j = row * xruns + xrun; pair x0 = 2 (BLOCK xrun + tid))
-    for (int32_t j = 0; j <= items; ++j) {
-        // ---- stage item j + 1 (j = -1 .. items - 1 in effect: the loop runs one ahead) ----
-        const int32_t jn = j;  // the item staged in this pass
-        if (jn < items) {
-            const int32_t rr = jn / xruns;
-            const int32_t row = row0 + rr;
-            const int32_t x0 = ((jn - rr * xruns) * BLOCK + tid) * 2;
-            const int32_t z = (int32_t)a.dny.div((uint32_t)row);
-            const int32_t y = row - z * ny;
-            if (!(y == 0 || y == ny - 1 || z == 0 || z == nz - 1 || x0 == 0 || x0 + 2 >= nx)) {
-                const int32_t idx0 = x0 + row * nx;
-                const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * 2;
-                const int b = jn & 1;
-                int k = Q;
-#pragma unroll
-                for (int i = 0; i < Q; ++i) {
-                    const char* w = fb + r.loff[i];  // the aligned pair (x0, x0 + 1) of the source row
-                    if (WT_PIPE_OK(1, w, f_lo, f_hi, 4)) cp_async4(&stage[b][i][tid], w);
-                    // the pair holding x0 - 1 (cx > 0) or x0 + 2 (cx < 0), inside the source row
-                    if (cx(i) > 0) {
-                        if (WT_PIPE_OK(2, w - 4, f_lo, f_hi, 4)) cp_async4(&stage[b][k][tid], w - 4);
-                        ++k;
-                    }
-                    if (cx(i) < 0) {
-                        if (WT_PIPE_OK(3, w + 4, f_lo, f_hi, 4)) cp_async4(&stage[b][k][tid], w + 4);
-                        ++k;
-                    }
-                }
-                const uint8_t* cw = a.code + (idx0 & ~3);
-                if (WT_PIPE_OK(4, cw, a.code, c_hi, 4)) cp_async4(&stage_code[b][tid], cw);
+    if constexpr (FUSE) {
+        if (valid && (y == ny - 2 || z == nz - 2)) {  // uniform over the block
+            if (y == ny - 2) fused_face_pair<PREC, FAST>(a, x0, ny - 1, z, m);
+            if (z == nz - 2) {
+                fused_face_pair<PREC, FAST>(a, x0, y, nz - 1, m);
+                if (y == 1) fused_face_pair<PREC, FAST>(a, x0, 0, nz - 1, m);
+                if (y == ny - 2) fused_face_pair<PREC, FAST>(a, x0, ny - 1, nz - 1, m);
             }
-        }
-        cp_async_commit();
-        if (j == 0) continue;
-        cp_async_wait1();  // this thread's copies of item j - 1 have landed
-        // ---- compute item jc = j - 1 from its stage ----
-        const int32_t jc = j - 1;
-        const int32_t rr = jc / xruns;
-        const int32_t row = row0 + rr;
-        const int32_t x0 = ((jc - rr * xruns) * BLOCK + tid) * 2;
-        const int32_t z = (int32_t)a.dny.div((uint32_t)row);
-        const int32_t y = row - z * ny;
-        const bool interior_row = !(y == 0 || y == ny - 1 || z == 0 || z == nz - 1);
-        const bool staged = interior_row && x0 > 0 && x0 + 2 < nx;
-        const int b = jc & 1;
-        const int32_t idx0 = x0 + row * nx;
-        const uint32_t codes = staged ? (stage_code[b][tid] >> (8 * (idx0 & 3))) & 0xffffu : 0xffffu;
-        if (!pure_pair(interior_row, staged, codes, x0, nx)) continue;  // left to k_step_rows
-        T f[2][Q];
-        int k = Q;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            S v[2], e[2];
-            const uint32_t w = stage[b][i][tid];
-            memcpy(v, &w, 4);
-            if (cx(i) == 0) {
-                f[0][i] = P::to(v[0]);
-                f[1][i] = P::to(v[1]);
-            } else {
-                const uint32_t wn = stage[b][k][tid];
-                ++k;
-                memcpy(e, &wn, 4);
-                if (cx(i) > 0) {
-                    f[0][i] = P::to(e[1]);  // x0 - 1
-                    f[1][i] = P::to(v[0]);
-                } else {
-                    f[0][i] = P::to(v[1]);
-                    f[1][i] = P::to(e[0]);  // x0 + 2
-                }
-            }
-        }
-        T m[2][4];
-        collide_two<P, FAST>(a, f, x0, m);
-        char* ob = reinterpret_cast<char*>(a.dst[0]) + (int64_t)idx0 * 2;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            uint32_t w;
-            if constexpr (std::is_same<S, __half>::value) {
-                const __half2 h = __floats2half2_rn(f[0][i], f[1][i]);
-                memcpy(&w, &h, 4);
-            } else {
-                const __nv_bfloat162 h = __floats2bfloat162_rn(f[0][i], f[1][i]);
-                memcpy(&w, &h, 4);
-            }
-            char* o = ob + r.soff[i];
-            if (WT_PIPE_OK(5, o, o_lo, o_hi, 4)) *reinterpret_cast<uint32_t*>(o) = w;
-        }
-        // mac where faces read it: a pure pair holds neither x = 1 nor x = nx - 2
-        if (a.mac_all || y == 1 || y == ny - 2 || z == 1 || z == nz - 2) {
-            store_mac(a.mac_cur, idx0, m[0][0], m[0][1], m[0][2], m[0][3]);
-            store_mac(a.mac_cur, idx0 + 1, m[1][0], m[1][1], m[1][2], m[1][3]);
         }
     }
 }

@@ -12,7 +12,8 @@ namespace wt {
 // cells (v cells per thread, block threads, minb resident blocks per SM, which bounds
 // registers); kind 1: streaming through shared memory (chunk cells per stage, stages
 // pipeline stages); kind 2: direct loads over a grid of lattice rows (one block row per
-// x-run of a lattice row, v = 2 cells per thread).
+// x-run of a lattice row, v = 2 cells per thread); kind 4: kind 2 with the later face cells
+// fused in (no separate face kernel).
 struct StepVariant {
     int id, kind, v, block, minb, chunk, stages;
     int (*launch)(const void* args, int32_t n, cudaStream_t st);

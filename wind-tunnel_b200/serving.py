@@ -116,10 +116,10 @@ class SessionServer:
         self.collision = collision
         self.period = 1.0 / fps
         self.steps_per_frame = int(steps_per_frame)
-        # batched tile: two cells per thread, 256 threads, 80 registers (the fastest batched
-        # shape in fp32 and fp16; the batch descriptor's fields take registers that a single
-        # tunnel's constant-bank parameters do not), one cell per thread for fp64
-        self.tile = int(tile) if tile else (2 if precision == 'fp64' else 7)
+        # batched tile of the persistent executor: the grid form of tile 3 (two cells per thread,
+        # 128 threads, one block per work-list tile), the fastest batched shape on config 4; one
+        # cell per thread for fp64
+        self.tile = int(tile) if tile else (2 if precision == 'fp64' else 103)
         # executor of the round's steps: every tunnel's own kernel on its own stream, all at
         # once ('streams', the faster on uneven mixes) or one persistent batched kernel
         self.batch_mode = batch_mode
