@@ -329,9 +329,10 @@ def run_ours(args, rank, world, local_rank):
 
 def run_batching(dev, replays=5, graph_steps=100):
     """Config 4: 24 tunnels (0.5M-8M cells, 2:1:1, own obstacles and flow parameters) in one
-    batch: persistent bulk kernel over a tile work-list plus a face kernel per step, captured
-    as a CUDA graph of `graph_steps` steps. The batch tile is picked by timing each batched
-    tile shape. The streams executor (every tunnel's own kernel on its own stream, forked and
+    batch: one bulk kernel over every tunnel plus a face kernel per step, captured as a CUDA
+    graph of `graph_steps` steps. The batch tile (a persistent work-list loop, one block per
+    work-list tile, or the tunnels' descriptors in the kernel parameters) is picked by timing
+    each batched tile shape. The streams executor (every tunnel's own kernel on its own stream, forked and
     joined inside one graph) is timed the same way. Every tunnel is then re-run alone for
     every step both executors made and compared bit for bit (populations, mac, forces), with
     its rate alone beside it."""
@@ -350,7 +351,8 @@ def run_batching(dev, replays=5, graph_steps=100):
     cells = sum(s.n for s in solvers)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tile_ms, steps_done = {}, 0
-    for tile in (3, 7, 18, 103, 104, 118):  # persistent forms, then the grid forms (100 + k)
+    # a persistent form, grid forms (100 + k), then the parameter-space forms (200 + k)
+    for tile in (7, 103, 118, 203, 218, 229):
         b = TunnelBatch(solvers, params, tile=tile)
         b.step(2)
         ev0.record(b.stream)

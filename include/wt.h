@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define WT_ABI_VERSION 3
+#define WT_ABI_VERSION 4
 
 enum {
     WT_OK = 0,
@@ -159,8 +159,12 @@ int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void*
  * results are bit-identical to stepping it alone with wt_step. All tunnels share precision and
  * collision form. tile selects the shape: a direct-load tile id k of wt_step_tiles (1-5, 7, 18)
  * runs as a persistent kernel (one wave of blocks looping over the work list); 100 + k (102,
- * 103, 104, 118) as one block per work-list tile; 0 = default. The caller allocates a 256-byte aligned device workspace of
- * wt_batch_workspace_bytes (descriptor table and work lists). cur gives each tunnel's
+ * 103, 104, 118) as one block per work-list tile; 200 + k (203, 204, 218, and 229, which is
+ * tile 18 with each pair's pull issued with its code bytes) with the tunnels' descriptors in
+ * the kernel parameters, one block per tile of BLOCK * V cells, groups of tunnels that fit the
+ * 32 KB parameter space per launch, and no device work list; 0 = default. The caller allocates
+ * a 256-byte aligned device workspace of wt_batch_workspace_bytes (descriptor table and work
+ * lists; 256 bytes, unused, for the 200 + k forms). cur gives each tunnel's
  * current population buffer at creation; wt_batch_cur reports it later. A batch must be
  * re-created after any of its tunnels is stepped on its own. */
 typedef struct wt_batch wt_batch;
@@ -169,6 +173,10 @@ int wt_batch_create(const wt_grid* grids, int32_t count, const double* uin, cons
                     const int32_t* cur, int32_t tile, void* workspace, int64_t workspace_bytes, void* stream,
                     wt_batch** out);
 int wt_batch_step(wt_batch* b, int32_t steps, int32_t flags, void* stream);
+/* Tunnel t advances steps[t] steps (0 leaves it as it is); WT_STEP_MAC_ALL_LAST applies to
+ * each tunnel's own last step. Uneven counts need a parameter-space tile (200 + k); the other
+ * forms accept equal counts only. */
+int wt_batch_step_each(wt_batch* b, const int32_t* steps, int32_t flags, void* stream);
 /* Capture `steps` (even) steps as a CUDA graph on a non-default stream; replay it with
  * wt_batch_replay (each replay advances every tunnel by `steps` steps). */
 int wt_batch_capture(wt_batch* b, int32_t steps, int32_t flags, void* stream);

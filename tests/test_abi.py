@@ -37,7 +37,7 @@ def test_exports_every_declared_symbol(L):
 
 
 def test_abi_version(L):
-    assert L.wt_abi_version() == W.ABI_VERSION == 3
+    assert L.wt_abi_version() == W.ABI_VERSION == 4
 
 
 @pytest.mark.parametrize('dims,ok', [((128, 64, 64), True), ((4, 3, 3), True), ((12, 8, 10), True),

@@ -134,7 +134,7 @@ def test_two_clients_over_websockets_match_their_sessions_alone():
         s0 = serving.Session(s.id, dims, np.zeros(int(np.prod(dims)), np.uint8), dict(server.ENGINE_PARAMS),
                              float('inf'), particles=0, frontal=1)
         s0.p['particles'] = server.ENGINE_PARAMS['particles']
-        want = _engine_replay(s0, script, 'fp32', 'streams', NFRAMES)
+        want = _engine_replay(s0, script, 'fp32', srv.steps_each, NFRAMES)
         assert len(got[k]) == NFRAMES
         for j, (a, b) in enumerate(zip(got[k], want)):
             assert a == b, f'client {k} frame {j} differs from its session run alone'

@@ -44,13 +44,16 @@ def _alone(s, frames, precision, k):
     return out
 
 
-@pytest.mark.parametrize('mode', ['streams', 'persistent'])
+EXECUTORS = [('streams', 0), ('persistent', 2), ('persistent', 229)]
+
+
+@pytest.mark.parametrize('mode,tile', EXECUTORS)
 @pytest.mark.parametrize('precision', ['fp32', 'fp16'])
-def test_each_session_same_alone_and_in_the_mix(precision, mode):
+def test_each_session_same_alone_and_in_the_mix(precision, mode, tile):
     import serving
     clock = Clock()
     srv = serving.SessionServer('cuda:0', budget_bytes=1e9, precision=precision, clock=clock, keep_frames=True,
-                                tile=2, batch_mode=mode, rate_in_header=False)
+                                tile=tile, batch_mode=mode, rate_in_header=False)
     ss = _sessions()
     srv.submit(ss[0])
     srv.submit(ss[1])
@@ -75,9 +78,10 @@ def test_each_session_same_alone_and_in_the_mix(precision, mode):
     srv.close()
 
 
-def _engine_replay(s0, script, precision, mode, rounds):
+def _engine_replay(s0, script, precision, each, rounds):
     """One session alone, driven as the reference Engine drives its Solver (server/app.py:
-    104-193): commands, then step(steps) when running, then a frame (Cp every third frame)."""
+    104-193): commands, then step(steps) when running, then a frame (Cp every third frame).
+    each: the session's own 'steps' per frame (else the server's 10)."""
     import gzip
     import numpy as np
     import wire
@@ -111,7 +115,7 @@ def _engine_replay(s0, script, precision, mode, rounds):
                 else:
                     sv.set_surface(got[1], got[2])
         running = bool(p.get('running', True))
-        k = (int(p.get('steps', 10)) if mode == 'streams' else 10) if running else 0
+        k = (int(p.get('steps', 10)) if each else 10) if running else 0
         if k:
             sv.step(k, p)
         frame_no += 1
@@ -124,8 +128,8 @@ def _engine_replay(s0, script, precision, mode, rounds):
     return frames
 
 
-@pytest.mark.parametrize('mode', ['streams', 'persistent'])
-def test_client_commands_match_the_engine_semantics(mode):
+@pytest.mark.parametrize('mode,tile', EXECUTORS)
+def test_client_commands_match_the_engine_semantics(mode, tile):
     """Two sessions under client pacing receive parameter changes, a reset, a respawn, a mask
     and a surface upload, a pause and a resume, through SessionServer.command; every frame
     equals the frame the same session gets alone when the same commands are applied the way
@@ -155,7 +159,7 @@ def test_client_commands_match_the_engine_semantics(mode):
     rounds = 7
     clock = Clock()
     srv = serving.SessionServer('cuda:0', budget_bytes=1e9, precision='fp32', clock=clock, keep_frames=True,
-                                batch_mode=mode, pacing='client', rate_in_header=False)
+                                tile=tile, batch_mode=mode, pacing='client', rate_in_header=False)
     for s in ss:
         srv.submit(s)
     for r in range(rounds):
@@ -171,7 +175,7 @@ def test_client_commands_match_the_engine_semantics(mode):
         got[sid].append(frame)
     srv.close()
     for s0 in originals:
-        want = _engine_replay(s0, script, 'fp32', mode, rounds)
+        want = _engine_replay(s0, script, 'fp32', srv.steps_each, rounds)
         assert len(got[s0.id]) == rounds
         for r, (a, b) in enumerate(zip(got[s0.id], want)):
             assert a == b, f'session {s0.id} frame {r}'

@@ -160,6 +160,10 @@ def test_oversubscribed_latency_is_round_time():
     # first round: requested at 0, ready at 0.6; afterwards each request waits one round
     assert st['p50_ms'] == pytest.approx(600.0)
     assert srv.cell_updates / (c.t - srv.t0) == pytest.approx(rate)  # the fake GPU never idles
+    slow = st['slow_rounds']  # the five rounds, longest first, then the median one
+    assert len(slow) == 6 and slow[-1]['median'] and all(r['sessions'] == 3 for r in slow)
+    assert [r['ms'] for r in slow[:5]] == sorted((r['ms'] for r in slow[:5]), reverse=True)
+    assert slow[-1]['ms'] == pytest.approx(600.0)
 
 
 def test_arrival_joins_next_round_and_batch_rebuilds():
@@ -276,12 +280,20 @@ def test_per_session_steps_with_the_streams_executor():
     srv.round()
     assert FakeBatch.steps == [[10, 4]]
     assert srv.active[1].solver.advanced == 4
-    p = _server(c, batch_mode='persistent')
+    # the parameter-space batched tiles (the default) step sessions by their own counts too
+    q = _server(c, batch_mode='persistent')
+    assert q.tile == 229 and q.steps_each
+    q.submit(_session(0, 2))
+    q.submit(_session(1, 2))
+    q.command(1, {'type': 'params', 'steps': 4})
+    q.round()
+    assert FakeBatch.steps == [[10, 4]]
+    p = _server(c, batch_mode='persistent', tile=103)
     p.submit(_session(0, 2))
     p.submit(_session(1, 2))
     p.command(1, {'type': 'params', 'steps': 4})
     p.round()
-    assert FakeBatch.steps == [10]  # one launch steps every tunnel alike
+    assert FakeBatch.steps == [10]  # one launch of a work-list tile steps every tunnel alike
 
 
 def test_surface_pressure_every_third_frame():

@@ -3,15 +3,19 @@
 ``TunnelBatch`` groups Solvers of one device, precision and collision form, in one of two
 executors:
 
-* ``mode='persistent'``: each step runs one persistent bulk kernel over a tile work-list that
-  spans every tunnel, then one kernel over all tunnels' face cells; ``capture(k)`` records k
-  (even) steps as a CUDA graph that ``replay()`` launches with a single call.
+* ``mode='persistent'``: each step runs one bulk kernel over every tunnel, then one kernel over
+  all tunnels' face cells; ``capture(k)`` records k (even) steps as a CUDA graph that
+  ``replay()`` launches with a single call. The tile picks the kernel's form: a persistent
+  loop over a device work list (tiles 1-5, 7, 18), one block per work-list tile (100 + k), or
+  the tunnels' descriptors in the kernel parameters (200 + k, no device work list; these also
+  step tunnels by different counts).
 * ``mode='streams'``: each tunnel is stepped by the single-tunnel kernel on its own stream, all
   streams running at once after the batch stream's prior work, and the batch stream joins them;
   ``capture(k)`` records that fork and join (k even) as one CUDA graph.
   Each kernel keeps its tunnel's scalars in its constant-bank parameters, so it runs the
-  64-register two-cell tile; concurrent tunnels fill each other's tails. On a mix of 0.5-33.5M
-  tunnels this executor is the faster one (fp16 60.6 vs 40.5 GLUPS).
+  64-register two-cell tile; concurrent tunnels fill each other's tails. On config 4 (24
+  tunnels of 0.5-8M cells) it runs as fast as the parameter-space tile 229 in fp32 and a little
+  slower in fp16, but it costs two launches per tunnel and step instead of two per step.
 
 Either way every tunnel's populations are bit-identical to stepping its Solver alone, the
 Solvers' ``cur`` is kept in sync, and ``event()`` orders later work after the steps. A
@@ -57,6 +61,7 @@ class TunnelBatch:
         self._smag = dbl(*[float(p['smag']) for p in params])
         self._cur = (ctypes.c_int32 * n)(*[s.cur for s in self.solvers])
         self.tile = int(tile)
+        self.steps_each = self.tile // 100 == 2  # per-tunnel step counts in one batch
         self.params = [dict(p) for p in params]
         self.cells = sum(s.n for s in self.solvers)
         self.handle = ctypes.c_void_p()
@@ -106,22 +111,27 @@ class TunnelBatch:
             raise MemberError(failed)
 
     def step(self, steps, mac_all_last=True):
-        """Advance every tunnel `steps` steps; with the streams executor `steps` may also be one
-        count per tunnel (each tunnel is its own launch)."""
-        if isinstance(steps, (list, tuple)):
+        """Advance every tunnel `steps` steps; `steps` may also be one count per tunnel with the
+        streams executor (each tunnel is its own launch) and with a parameter-space tile
+        (200 + k: each step launches the tunnels with steps to go)."""
+        each = isinstance(steps, (list, tuple))
+        if each:
             if len(steps) != len(self.solvers):
                 raise ValueError('one step count per tunnel')
             counts = [int(k) for k in steps]
-            if self.mode != 'streams' and len(set(counts)) > 1:
-                raise ValueError('the persistent executor steps every tunnel alike')
+            if self.mode != 'streams' and len(set(counts)) > 1 and not self.steps_each:
+                raise ValueError(f'batched tile {self.tile} steps every tunnel alike (a 200 + k tile does not)')
         else:
             counts = [int(steps)] * len(self.solvers)
         if self.mode == 'streams':
             self._step_streams(counts, mac_all_last)
             return
-        steps = counts[0]
         self._wait_members()
-        call('wt_batch_step', self.handle, int(steps), W.STEP_MAC_ALL_LAST if mac_all_last else 0, self.sh)
+        flags = W.STEP_MAC_ALL_LAST if mac_all_last else 0
+        if each:
+            call('wt_batch_step_each', self.handle, (ctypes.c_int32 * len(counts))(*counts), flags, self.sh)
+        else:
+            call('wt_batch_step', self.handle, counts[0], flags, self.sh)
         self._sync_cur()
 
     def _capture_streams(self, steps, mac_all_last):

@@ -1,11 +1,13 @@
 // Many tunnels of uneven sizes advanced together: one bulk kernel over a tile work-list
 // spanning every tunnel, then one face kernel over all tunnels' face cells, per step; optionally
-// captured as a CUDA graph of an even number of steps and replayed. The kernels come in two
-// forms (wt_kernels.cuh): persistent (one wave of blocks looping over the lists) and grid (one
+// captured as a CUDA graph of an even number of steps and replayed. The kernels come in three
+// forms (wt_kernels.cuh): persistent (one wave of blocks looping over the lists), grid (one
 // block per sub-tile of the lists, tile ids 100 + k), which fits the 64 registers of the
-// single-tunnel two-cell tile.
+// single-tunnel two-cell tile, and parameter-space (tile ids 200 + k: the descriptors travel in
+// the kernel arguments, groups of up to BatchParams::MAXT tunnels per launch, and the device
+// workspace is unused).
 //
-// Device workspace (caller-allocated, wt_batch_workspace_bytes):
+// Device workspace of the first two forms (caller-allocated, wt_batch_workspace_bytes):
 //   desc  -- 4 StepArgs per tunnel, indexed [tunnel][parity][mac_all]: parity p holds the
 //            tunnel's buffers for cur = cur0 ^ p, so all tunnels flip together;
 //   bulk  -- work items {tunnel, first cell} of BLOCK * V * ITEM_SUB cells each;
@@ -33,6 +35,10 @@ struct wt_batch {
     int2* faces;
     int32_t n_bulk, n_faces;
     int grid_bulk, grid_faces;
+    std::vector<unsigned char> pdesc;  // parameter-space form: descriptors [parity][mac_all][tunnel]
+    std::vector<int32_t> par;          // parameter-space form: tunnel t's current buffer is cur0[t] ^ par[t]
+    std::vector<unsigned char> group;  // parameter-space form: one step's descriptors, gathered
+    size_t desc_bytes;
     cudaGraphExec_t graph;
     int32_t graph_steps;
 };
@@ -58,9 +64,9 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 // tile shape of a batch (direct-load variants only; 100 + k is the grid form of tile k)
 int tile_shape(int32_t tile, int* v, int* block) {
-    static const int ids[][3] = {{1, 1, 256},   {2, 1, 128},   {3, 2, 128},   {4, 2, 128},  {5, 4, 128},
+    static const int ids[][3] = {{1, 1, 256},   {2, 1, 128},   {3, 2, 128},   {4, 2, 128},   {5, 4, 128},
                                  {7, 2, 256},   {18, 2, 128},  {102, 1, 128}, {103, 2, 128}, {104, 2, 128},
-                                 {118, 2, 128}};
+                                 {118, 2, 128}, {203, 2, 128}, {204, 2, 128}, {218, 2, 128}, {229, 2, 128}};
     const int want = tile > 0 ? tile : 2;
     for (const auto& r : ids)
         if (r[0] == want) {
@@ -122,7 +128,38 @@ void fill_desc(const wt_grid& g, int32_t cur0, double uin, double tau, double sm
     std::memcpy(out, &a, sizeof(a));
 }
 
+// Parameter-space form: tunnel t advances each[t] steps (all `steps` when each is null). Step s
+// launches the tunnels with more than s steps to go, each with the descriptor of its own
+// parity, so tunnels with different counts keep their own buffer parity.
+int launch_params(wt_batch* b, const int32_t* each, int32_t steps, int32_t flags, cudaStream_t st) {
+    int32_t smax = steps;
+    if (each) {
+        smax = 0;
+        for (int32_t t = 0; t < b->count; ++t) smax = std::max(smax, each[t]);
+    }
+    const size_t ds = b->desc_bytes;
+    b->group.resize((size_t)b->count * ds);
+    for (int32_t s = 0; s < smax; ++s) {
+        int32_t m = 0;
+        for (int32_t t = 0; t < b->count; ++t) {
+            const int32_t k = each ? each[t] : steps;
+            if (s >= k) continue;
+            const int parity = (b->par[t] + s) & 1;
+            const int mac_all = (flags & WT_STEP_MAC_ALL_LAST) && s == k - 1;
+            std::memcpy(b->group.data() + (size_t)m * ds,
+                        b->pdesc.data() + ((size_t)(parity * 2 + mac_all) * b->count + t) * ds, ds);
+            ++m;
+        }
+        if (int rc = b->var->bulk_p(b->group.data(), m, st)) return rc;
+        if (int rc = b->var->faces_p(b->group.data(), m, st)) return rc;
+    }
+    if (int rc = wt_cuda_check("wt_batch step launch")) return rc;
+    for (int32_t t = 0; t < b->count; ++t) b->par[t] ^= (each ? each[t] : steps) & 1;
+    return WT_OK;
+}
+
 int launch_steps(wt_batch* b, int32_t steps, int32_t flags, cudaStream_t st) {
+    if (b->var->form == BATCH_PARAMS) return launch_params(b, nullptr, steps, flags, st);
     for (int32_t s = 0; s < steps; ++s) {
         const int parity = (b->base + s) & 1;
         const int mac_all = (flags & WT_STEP_MAC_ALL_LAST) && s == steps - 1;
@@ -130,7 +167,9 @@ int launch_steps(wt_batch* b, int32_t steps, int32_t flags, cudaStream_t st) {
         b->var->bulk(&args, b->grid_bulk, st);
         b->var->faces(&args, b->grid_faces, st);
     }
-    return wt_cuda_check("wt_batch step launch");
+    if (int rc = wt_cuda_check("wt_batch step launch")) return rc;
+    b->base ^= steps & 1;
+    return WT_OK;
 }
 
 }  // namespace
@@ -141,6 +180,7 @@ extern "C" int64_t wt_batch_workspace_bytes(const wt_grid* grids, int32_t count,
     if (!tile_shape(tile, &v, &block)) return wt_set_error(WT_ERR_ARG, "wt_batch: tile %d has no batched form", tile);
     const size_t ds = desc_bytes_for(grids[0].precision);
     if (!ds) return wt_set_error(WT_ERR_ARG, "wt_batch: unknown precision %d", grids[0].precision);
+    if (tile / 100 == 2) return 256;  // parameter-space form: nothing on the device
     int64_t nb, nf;
     work_counts(grids, count, v * block * ITEM_SUB, &nb, &nf);
     return (int64_t)(align256(4 * ds * count) + align256(8 * nb) + align256(8 * nf));
@@ -184,6 +224,37 @@ extern "C" int wt_batch_create(const wt_grid* grids, int32_t count, const double
         return wt_set_error(WT_ERR_ARG, "wt_batch_create: workspace not 256-byte aligned");
 
     const size_t ds = desc_bytes_for(prec);
+    if (var->form == BATCH_PARAMS) {
+        wt_batch* b = new wt_batch();
+        b->precision = prec;
+        b->collision = coll;
+        b->count = count;
+        b->base = 0;
+        b->cur0.assign(cur, cur + count);
+        b->var = var;
+        b->desc = nullptr;
+        b->bulk = b->faces = nullptr;
+        b->n_bulk = b->n_faces = 0;
+        b->grid_bulk = b->grid_faces = 0;
+        b->desc_bytes = ds;
+        b->par.assign(count, 0);
+        b->pdesc.assign((size_t)4 * count * ds, 0);
+        for (int32_t t = 0; t < count; ++t)
+            for (int p = 0; p < 2; ++p)
+                for (int m = 0; m < 2; ++m) {
+                    void* dst = b->pdesc.data() + ((size_t)(p * 2 + m) * count + t) * ds;
+                    switch (prec) {
+                        case WT_F32: fill_desc<WT_F32>(grids[t], cur[t], uin[t], tau[t], smag[t], p, m, dst); break;
+                        case WT_F16: fill_desc<WT_F16>(grids[t], cur[t], uin[t], tau[t], smag[t], p, m, dst); break;
+                        case WT_BF16: fill_desc<WT_BF16>(grids[t], cur[t], uin[t], tau[t], smag[t], p, m, dst); break;
+                        case WT_F64: fill_desc<WT_F64>(grids[t], cur[t], uin[t], tau[t], smag[t], p, m, dst); break;
+                    }
+                }
+        b->graph = nullptr;
+        b->graph_steps = 0;
+        *out = b;
+        return WT_OK;
+    }
     int64_t nb, nf;
     work_counts(grids, count, v * block * ITEM_SUB, &nb, &nf);
     std::vector<unsigned char> host(need, 0);
@@ -224,13 +295,14 @@ extern "C" int wt_batch_create(const wt_grid* grids, int32_t count, const double
     b->faces = reinterpret_cast<int2*>(static_cast<unsigned char*>(workspace) + align256(4 * ds * count) + align256(8 * nb));
     b->n_bulk = (int32_t)nb;
     b->n_faces = (int32_t)nf;
-    if (var->persistent) {  // one wave of blocks looping over the lists
+    if (var->form == BATCH_PERSISTENT) {  // one wave of blocks looping over the lists
         b->grid_bulk = (int)std::min<int64_t>(nb, (int64_t)num_sms() * var->minb);
         b->grid_faces = (int)std::min<int64_t>(nf, (int64_t)num_sms() * 8);
     } else {  // one block per sub-tile
         b->grid_bulk = (int)(nb * ITEM_SUB);
         b->grid_faces = (int)(nf * ITEM_SUB);
     }
+    b->desc_bytes = ds;
     b->graph = nullptr;
     b->graph_steps = 0;
     *out = b;
@@ -240,9 +312,22 @@ extern "C" int wt_batch_create(const wt_grid* grids, int32_t count, const double
 extern "C" int wt_batch_step(wt_batch* b, int32_t steps, int32_t flags, void* stream) {
     if (!b) return wt_set_error(WT_ERR_ARG, "wt_batch_step: null batch");
     if (steps < 0) return wt_set_error(WT_ERR_ARG, "wt_batch_step: steps < 0");
-    if (int rc = launch_steps(b, steps, flags, static_cast<cudaStream_t>(stream))) return rc;
-    b->base ^= steps & 1;
-    return WT_OK;
+    return launch_steps(b, steps, flags, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int wt_batch_step_each(wt_batch* b, const int32_t* steps, int32_t flags, void* stream) {
+    if (!b || !steps) return wt_set_error(WT_ERR_ARG, "wt_batch_step_each: null argument");
+    bool uniform = true;
+    for (int32_t t = 0; t < b->count; ++t) {
+        if (steps[t] < 0) return wt_set_error(WT_ERR_ARG, "wt_batch_step_each: steps of tunnel %d < 0", t);
+        uniform = uniform && steps[t] == steps[0];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (b->var->form == BATCH_PARAMS) return launch_params(b, steps, 0, flags, st);
+    if (!uniform)
+        return wt_set_error(WT_ERR_ARG, "wt_batch_step_each: tile %d steps every tunnel alike (use a 200 + k tile)",
+                            b->var->id);
+    return launch_steps(b, steps[0], flags, st);
 }
 
 extern "C" int wt_batch_capture(wt_batch* b, int32_t steps, int32_t flags, void* stream) {
@@ -284,7 +369,8 @@ extern "C" int wt_batch_replay(wt_batch* b, void* stream) {
 
 extern "C" int wt_batch_cur(const wt_batch* b, int32_t* cur_out) {
     if (!b || !cur_out) return wt_set_error(WT_ERR_ARG, "wt_batch_cur: null argument");
-    for (int32_t t = 0; t < b->count; ++t) cur_out[t] = b->cur0[t] ^ b->base;
+    for (int32_t t = 0; t < b->count; ++t)
+        cur_out[t] = b->cur0[t] ^ (b->var->form == BATCH_PARAMS ? b->par[t] : b->base);
     return WT_OK;
 }
 

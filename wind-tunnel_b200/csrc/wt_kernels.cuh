@@ -11,12 +11,12 @@ namespace wt {
 
 // ---- single tunnel ----
 
-template <int PREC, bool FAST, int V, int BLOCK, int MINB>
+template <int PREC, bool FAST, int V, int BLOCK, int MINB, bool EARLY = false>
 static int launch_bulk(const void* args, int32_t n, cudaStream_t st) {
     using P = Prec<PREC>;
     const auto& a = *static_cast<const StepArgs<typename P::S, typename P::T>*>(args);
     const int32_t nthreads = n / V;
-    k_step_bulk<PREC, FAST, V, BLOCK, MINB><<<(unsigned)((nthreads + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
+    k_step_bulk<PREC, FAST, V, BLOCK, MINB, EARLY><<<(unsigned)((nthreads + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
     return WT_OK;
 }
 
@@ -40,7 +40,7 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
     return WT_OK;
 }
 
-template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false>
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false, bool EARLY = false>
 static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     using P = Prec<PREC>;
     using S = typename P::S;
@@ -56,7 +56,7 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
         r.soff[i] = (int64_t)i * a.n * (int64_t)sizeof(S);
     }
     const dim3 grid((unsigned)((a.nx / 2 + BLOCK - 1) / BLOCK), (unsigned)a.ny, (unsigned)a.nz);
-    k_step_rows<PREC, FAST, BLOCK, MINB, ADDR, FUSE><<<grid, BLOCK, 0, st>>>(r);
+    k_step_rows<PREC, FAST, BLOCK, MINB, ADDR, FUSE, EARLY><<<grid, BLOCK, 0, st>>>(r);
     return WT_OK;
 }
 
@@ -66,7 +66,9 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
 // thread, threads per block, minimum resident blocks per SM, and in the last field the
 // addressing form (0: per-population bases, 1: one base plus byte offsets); kind 4 is the row
 // grid with the face cells of k_step_faces computed by the blocks of the rows they read
-// (k_step_rows with FUSE), so the step is one kernel. wt_grid.tile
+// (k_step_rows with FUSE), so the step is one kernel. Tiles 29-32 issue each pair's pull
+// together with its code bytes instead of after them (EARLY): 29 is tile 18 so, 30-32 are
+// tiles 19, 21 and 22. wt_grid.tile
 // selects one (0 = the default for the precision and collision form); autotune.py times them.
 #define WT_VARIANTS(PREC, FAST)                                                          \
     {1, 0, 1, 256, 4, 0, 0, launch_bulk<PREC, FAST, 1, 256, 4>},                         \
@@ -96,7 +98,11 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     {25, 2, 2, 128, 9, 0, 0, launch_rows<PREC, FAST, 128, 9, 0>},                        \
     {26, 2, 2, 128, 10, 0, 0, launch_rows<PREC, FAST, 128, 10, 0>},                      \
     {27, 4, 2, 128, 8, 0, 0, launch_rows<PREC, FAST, 128, 8, 0, true>},                  \
-    {28, 4, 2, 64, 16, 0, 0, launch_rows<PREC, FAST, 64, 16, 0, true>}
+    {28, 4, 2, 64, 16, 0, 0, launch_rows<PREC, FAST, 64, 16, 0, true>},                 \
+    {29, 0, 2, 128, 8, 0, 0, launch_bulk<PREC, FAST, 2, 128, 8, true>},                  \
+    {30, 2, 2, 128, 8, 0, 0, launch_rows<PREC, FAST, 128, 8, 0, false, true>},           \
+    {31, 2, 2, 64, 16, 0, 0, launch_rows<PREC, FAST, 64, 16, 0, false, true>},           \
+    {32, 2, 2, 64, 16, 0, 1, launch_rows<PREC, FAST, 64, 16, 1, false, true>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants_of(int* count) {
@@ -112,15 +118,16 @@ const StepVariant* step_variants(bool fast, int* count) {
 
 // defaults until the autotuner has measured the tunnel (the fastest shapes at 33.5M cells):
 // two cells per thread at 64 registers, as the one-dimensional tile 18 for fp32 and the
-// reference-order collision, as the row-grid tile 21 (64 threads, 16 blocks per SM) for fp16 /
-// bf16 storage with the moment-space collision; fp64 needs 128 registers to avoid spills, so
-// it keeps two cells per thread at 128 registers (tile 4)
+// reference-order collision, as the row-grid tile 31 (64 threads, 16 blocks per SM, each pull
+// issued with its code bytes) for fp16 / bf16 storage with the moment-space collision; fp64
+// needs 128 registers to avoid spills, so it keeps two cells per thread at 128 registers
+// (tile 4)
 template <int PREC>
 const StepVariant* pick_variant(const wt_grid* g) {
     int count;
     const bool fast = g->collision == WT_COLLIDE_FAST;
     const StepVariant* t = step_variants<PREC>(fast, &count);
-    const int dflt = PREC == WT_F64 ? 4 : ((PREC == WT_F16 || PREC == WT_BF16) && fast ? 21 : 18);
+    const int dflt = PREC == WT_F64 ? 4 : ((PREC == WT_F16 || PREC == WT_BF16) && fast ? 31 : 18);
     const int want = g->tile > 0 ? g->tile : dflt;
     for (int k = 0; k < count; ++k) {
         if (t[k].id != want) continue;
@@ -272,20 +279,95 @@ static void launch_batch_faces(const void* args, int grid, cudaStream_t st) {
     k_batch_faces<PREC><<<grid, FACE_BLOCK, 0, st>>>(*static_cast<const BatchArgs*>(args));
 }
 
+// Parameter-space forms: the descriptors of up to MAXT tunnels and each tunnel's first block
+// (prefix sums of its block counts) are the kernel's argument, read through the constant bank;
+// block b belongs to the last tunnel t with first[t] <= b. No load of a work item or a
+// descriptor stands between a block's start and its pull.
+template <class S, class T>
+struct BatchParams {
+    static constexpr int MAXT = (32764 - 16) / (int)(sizeof(StepArgs<S, T>) + 4);
+    int32_t count;
+    int32_t first[MAXT + 1];
+    StepArgs<S, T> args[MAXT];
+};
+
+template <class BP>
+__device__ __forceinline__ int32_t param_tunnel(const BP& bp, int32_t b) {
+    int32_t lo = 0, hi = bp.count - 1;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi + 1) >> 1;
+        if (bp.first[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int PREC, bool FAST, int V, int BLOCK, int MINB, bool EARLY>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_batch_bulk_params(const __grid_constant__ BatchParams<typename Prec<PREC>::S, typename Prec<PREC>::T> bp) {
+    const int32_t b = (int32_t)blockIdx.x;
+    const int32_t t = param_tunnel(bp, b);
+    const auto& a = bp.args[t];
+    const int32_t idx0 = ((b - bp.first[t]) * BLOCK + (int32_t)threadIdx.x) * V;
+    bulk_cells<PREC, FAST, V, EARLY>(a, idx0, idx0 < a.n);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(FACE_BLOCK)
+    k_batch_faces_params(const __grid_constant__ BatchParams<typename Prec<PREC>::S, typename Prec<PREC>::T> bp) {
+    const int32_t b = (int32_t)blockIdx.x;
+    const int32_t t = param_tunnel(bp, b);
+    face_cell<PREC>(bp.args[t], (b - bp.first[t]) * FACE_BLOCK + (int32_t)threadIdx.x);
+}
+
+// FACES: the face kernel (FACE_BLOCK face cells per block) instead of the bulk one
+template <int PREC, bool FAST, int V, int BLOCK, int MINB, bool EARLY, bool FACES>
+static int launch_batch_params(const void* descs, int32_t count, cudaStream_t st) {
+    using S = typename Prec<PREC>::S;
+    using T = typename Prec<PREC>::T;
+    using BP = BatchParams<S, T>;
+    static_assert(sizeof(BP) <= 32764, "kernel parameters are limited to 32764 bytes");
+    const StepArgs<S, T>* d = static_cast<const StepArgs<S, T>*>(descs);
+    BP bp;
+    for (int32_t g0 = 0; g0 < count; g0 += BP::MAXT) {
+        const int32_t gc = std::min<int32_t>(count - g0, BP::MAXT);
+        bp.count = gc;
+        bp.first[0] = 0;
+        for (int32_t t = 0; t < gc; ++t) {
+            const StepArgs<S, T>& a = d[g0 + t];
+            bp.args[t] = a;
+            const int64_t cells = FACES ? (int64_t)a.nxy + (int64_t)a.nx * (a.nz - 2) : (int64_t)a.n;
+            const int64_t per = FACES ? FACE_BLOCK : (int64_t)BLOCK * V;
+            bp.first[t + 1] = bp.first[t] + (int32_t)((cells + per - 1) / per);
+        }
+        if constexpr (FACES) k_batch_faces_params<PREC><<<(unsigned)bp.first[gc], FACE_BLOCK, 0, st>>>(bp);
+        else k_batch_bulk_params<PREC, FAST, V, BLOCK, MINB, EARLY><<<(unsigned)bp.first[gc], BLOCK, 0, st>>>(bp);
+    }
+    return WT_OK;
+}
+
 // the direct-load tile shapes of wt_step, same ids, as persistent kernels; ids 100 + k are
-// the grid forms of tile k
+// the grid forms of tile k, ids 200 + k the parameter-space forms (229: tile 18 with the pull
+// issued with the code bytes, as single-tunnel tile 29)
+#define WT_BATCH_P(PREC, FAST, V, BLOCK, MINB, EARLY)                                                        \
+    nullptr, nullptr, launch_batch_params<PREC, FAST, V, BLOCK, MINB, EARLY, false>,                          \
+        launch_batch_params<PREC, FAST, V, BLOCK, MINB, EARLY, true>
 #define WT_BATCH_VARIANTS(PREC, FAST)                                                                        \
-    {1, 1, 256, 4, true, launch_batch_bulk<PREC, FAST, 1, 256, 4>, launch_batch_faces<PREC>},                \
-    {2, 1, 128, 8, true, launch_batch_bulk<PREC, FAST, 1, 128, 8>, launch_batch_faces<PREC>},                \
-    {3, 2, 128, 6, true, launch_batch_bulk<PREC, FAST, 2, 128, 6>, launch_batch_faces<PREC>},                \
-    {4, 2, 128, 4, true, launch_batch_bulk<PREC, FAST, 2, 128, 4>, launch_batch_faces<PREC>},                \
-    {5, 4, 128, 4, true, launch_batch_bulk<PREC, FAST, 4, 128, 4>, launch_batch_faces<PREC>},                \
-    {7, 2, 256, 3, true, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>},                \
-    {18, 2, 128, 8, true, launch_batch_bulk<PREC, FAST, 2, 128, 8>, launch_batch_faces<PREC>},               \
-    {102, 1, 128, 8, false, launch_batch_bulk_grid<PREC, FAST, 1, 128, 8>, launch_batch_faces_grid<PREC>},   \
-    {103, 2, 128, 6, false, launch_batch_bulk_grid<PREC, FAST, 2, 128, 6>, launch_batch_faces_grid<PREC>},   \
-    {104, 2, 128, 4, false, launch_batch_bulk_grid<PREC, FAST, 2, 128, 4>, launch_batch_faces_grid<PREC>},   \
-    {118, 2, 128, 8, false, launch_batch_bulk_grid<PREC, FAST, 2, 128, 8>, launch_batch_faces_grid<PREC>}
+    {1, 1, 256, 4, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 1, 256, 4>, launch_batch_faces<PREC>},    \
+    {2, 1, 128, 8, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 1, 128, 8>, launch_batch_faces<PREC>},    \
+    {3, 2, 128, 6, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 2, 128, 6>, launch_batch_faces<PREC>},    \
+    {4, 2, 128, 4, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 2, 128, 4>, launch_batch_faces<PREC>},    \
+    {5, 4, 128, 4, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 4, 128, 4>, launch_batch_faces<PREC>},    \
+    {7, 2, 256, 3, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 2, 256, 3>, launch_batch_faces<PREC>},    \
+    {18, 2, 128, 8, BATCH_PERSISTENT, launch_batch_bulk<PREC, FAST, 2, 128, 8>, launch_batch_faces<PREC>},   \
+    {102, 1, 128, 8, BATCH_GRID, launch_batch_bulk_grid<PREC, FAST, 1, 128, 8>, launch_batch_faces_grid<PREC>}, \
+    {103, 2, 128, 6, BATCH_GRID, launch_batch_bulk_grid<PREC, FAST, 2, 128, 6>, launch_batch_faces_grid<PREC>}, \
+    {104, 2, 128, 4, BATCH_GRID, launch_batch_bulk_grid<PREC, FAST, 2, 128, 4>, launch_batch_faces_grid<PREC>}, \
+    {118, 2, 128, 8, BATCH_GRID, launch_batch_bulk_grid<PREC, FAST, 2, 128, 8>, launch_batch_faces_grid<PREC>}, \
+    {203, 2, 128, 6, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 6, false)},                                \
+    {204, 2, 128, 4, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 4, false)},                                \
+    {218, 2, 128, 8, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 8, false)},                                \
+    {229, 2, 128, 8, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 8, true)}
 
 template <int PREC, bool FAST>
 const BatchVariant* batch_variant_of(int id) {

@@ -964,7 +964,20 @@ __device__ __forceinline__ void interior_pair(const StepArgs<typename Prec<PREC>
     interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, mo);
 }
 
-template <int PREC, bool FAST, int V>
+// interior_pair with the pull issued together with the code bytes instead of after them, so
+// the two loads' latencies overlap; an all-solid pair pulls too (and discards it)
+template <int PREC, bool FAST>
+__device__ __forceinline__ void interior_pair_early(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
+                                                    int32_t idx0, int32_t x0, int32_t y, int32_t z, bool row_shell) {
+    using P = Prec<PREC>;
+    typename P::T f[2][Q], mo[2][4];
+    PairRaw<typename P::S> r;
+    pair_load<PREC>(a, idx0, r);
+    pair_unpack<P, FAST>(a, r, f);
+    pair_finish<PREC, FAST>(a, idx0, x0, y, z, r.codes, row_shell, f, mo);
+}
+
+template <int PREC, bool FAST, int V, bool EARLY = false>
 __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& a,
                                            int32_t idx0, bool valid) {
     using P = Prec<PREC>;
@@ -977,6 +990,12 @@ __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S
     const int32_t y = row - z * ny;
     const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
     const bool row_shell = !face_row && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
+    if constexpr (V == 2 && EARLY) {
+        if (valid && !face_row) {
+            interior_pair_early<PREC, FAST>(a, idx0, x0, y, z, row_shell);
+            return;
+        }
+    }
     T mx = (T)0.0, my = (T)0.0, mz = (T)0.0, mr = (T)1.0;  // macro values of the latest cell
     uint32_t codes = 0;
     if (valid) {
@@ -1043,10 +1062,10 @@ __device__ __forceinline__ void bulk_cells(const StepArgs<typename Prec<PREC>::S
     }
 }
 
-template <int PREC, bool FAST, int V, int BLOCK, int MINB>
+template <int PREC, bool FAST, int V, int BLOCK, int MINB, bool EARLY = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_bulk(const StepArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> a) {
     const int32_t idx0 = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x) * V;
-    bulk_cells<PREC, FAST, V>(a, idx0, idx0 < a.n);
+    bulk_cells<PREC, FAST, V, EARLY>(a, idx0, idx0 < a.n);
 }
 
 // Face cell number t of the tunnel's k_step_faces set (z = nz-1 plane, then the y = ny-1
@@ -1241,7 +1260,25 @@ __device__ __forceinline__ void fused_face_pair(const StepArgs<typename Prec<PRE
     }
 }
 
-template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false>
+// The pull of a pair of an interior row in the lean path's addressing (ADDR), with the pair's
+// code bytes: the same values as pair_load.
+template <int PREC, int ADDR>
+__device__ __forceinline__ void pair_load_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
+                                               int32_t idx0, PairRaw<typename Prec<PREC>::S>& o) {
+    using S = typename Prec<PREC>::S;
+    const auto& a = r.a;
+    o.codes = *reinterpret_cast<const uint16_t*>(a.code + idx0);
+    const char* fb = reinterpret_cast<const char*>(a.fin) + (int64_t)idx0 * (int64_t)sizeof(S);
+    unroll<0, Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const S* p = ADDR == 0 ? a.src[i] + idx0 + cx(i) : reinterpret_cast<const S*>(fb + r.loff[i]);
+        o.v[i] = vload<S, 2>(p);
+        if constexpr (cx(i) > 0) o.e[i] = p[-1];
+        if constexpr (cx(i) < 0) o.e[i] = p[2];
+    });
+}
+
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false, bool EARLY = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
     using T = typename Prec<PREC>::T;
     const auto& a = r.a;
@@ -1255,13 +1292,33 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typenam
         return;
     }
     const bool row_shell = y == 1 || y == ny - 2 || z == 1 || z == nz - 2;
-    const uint32_t codes = valid ? *reinterpret_cast<const uint16_t*>(a.code + idx0) : 0xffffu;
     T m[2][4];
-    // lean unless a cell of the warp is solid (or past the row's end)
-    if (__all_sync(0xffffffffu, (codes & (CODE_SOLID * 0x0101u)) == 0)) {
-        pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell, m);
-    } else if (valid) {
-        interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, m);
+    if constexpr (EARLY) {
+        // the pull goes out with the code bytes, not after the vote on them, so the two loads'
+        // latencies overlap; both paths take the same pulled values
+        PairRaw<typename Prec<PREC>::S> pr;
+        uint32_t codes = 0xffffu;
+        if (valid) {
+            pair_load_rows<PREC, ADDR>(r, idx0, pr);
+            codes = pr.codes;
+        }
+        if (__all_sync(0xffffffffu, (codes & (CODE_SOLID * 0x0101u)) == 0)) {
+            T f[2][Q];
+            pair_unpack<Prec<PREC>, FAST>(a, pr, f);
+            pair_lean_finish<PREC, FAST>(r, f, idx0, x0, y, z, codes, row_shell, ADDR == 1, m);
+        } else if (valid) {
+            T f[2][Q];
+            pair_unpack<Prec<PREC>, FAST>(a, pr, f);  // an all-solid pair's values go unused
+            pair_finish<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, f, m);
+        }
+    } else {
+        const uint32_t codes = valid ? *reinterpret_cast<const uint16_t*>(a.code + idx0) : 0xffffu;
+        // lean unless a cell of the warp is solid (or past the row's end)
+        if (__all_sync(0xffffffffu, (codes & (CODE_SOLID * 0x0101u)) == 0)) {
+            pair_lean<PREC, FAST, ADDR>(r, idx0, x0, y, z, codes, row_shell, m);
+        } else if (valid) {
+            interior_pair<PREC, FAST>(a, idx0, x0, y, z, codes, row_shell, m);
+        }
     }
     if constexpr (FUSE) {
         if (valid && (y == ny - 2 || z == nz - 2)) {  // uniform over the block

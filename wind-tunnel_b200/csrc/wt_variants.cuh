@@ -19,13 +19,21 @@ struct StepVariant {
     int (*launch)(const void* args, int32_t n, cudaStream_t st);
 };
 
-// One tile shape of the batched bulk kernel and its face kernel. persistent: a grid of one
-// wave whose blocks loop over the work list; otherwise one block per sub-tile of the list.
+// One tile shape of the batched bulk kernel and its face kernel, in one of three forms:
+// BATCH_PERSISTENT -- a grid of one wave whose blocks loop over the device work list;
+// BATCH_GRID -- one block per sub-tile of the device work list;
+// BATCH_PARAMS -- no device work list: the tunnels' descriptors and block counts travel in the
+// kernel's parameter space (up to 32 KB), each block finds its tunnel there, and a batch larger
+// than one parameter block is launched in groups (bulk_p / faces_p take the host copies of the
+// count descriptors of this step's parity).
+enum BatchForm { BATCH_PERSISTENT = 0, BATCH_GRID = 1, BATCH_PARAMS = 2 };
 struct BatchVariant {
     int id, v, block, minb;
-    bool persistent;
+    int form;
     void (*bulk)(const void* args, int grid, cudaStream_t st);
     void (*faces)(const void* args, int grid, cudaStream_t st);
+    int (*bulk_p)(const void* descs, int32_t count, cudaStream_t st);
+    int (*faces_p)(const void* descs, int32_t count, cudaStream_t st);
 };
 
 // A batch work item is ITEM_SUB sub-tiles: BLOCK * V * ITEM_SUB cells of one tunnel (bulk) or

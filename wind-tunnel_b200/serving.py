@@ -116,13 +116,15 @@ class SessionServer:
         self.collision = collision
         self.period = 1.0 / fps
         self.steps_per_frame = int(steps_per_frame)
-        # batched tile of the persistent executor: the grid form of tile 3 (two cells per thread,
-        # 128 threads, one block per work-list tile), the fastest batched shape on config 4; one
-        # cell per thread for fp64
-        self.tile = int(tile) if tile else (2 if precision == 'fp64' else 103)
+        # batched tile of the library executor: the parameter-space form of the two-cell tile
+        # with early pulls (229; 204, at 128 registers, for fp64), the fastest batched shape on
+        # config 4, which also steps sessions by their own counts
+        self.tile = int(tile) if tile else (204 if precision == 'fp64' else 229)
         # executor of the round's steps: every tunnel's own kernel on its own stream, all at
-        # once ('streams', the faster on uneven mixes) or one persistent batched kernel
+        # once ('streams'), or the library's batched kernels ('persistent': two launches per
+        # step for all sessions)
         self.batch_mode = batch_mode
+        self.steps_each = batch_mode == 'streams' or self.tile // 100 == 2
         self.clock = clock
         self.solver_factory = solver_factory or self._make_solver
         self.batch_factory = batch_factory or self._make_batch
@@ -178,6 +180,9 @@ class SessionServer:
         self._stream = None
         self.phase = {'admit': 0.0, 'rebuild': 0.0, 'issue': 0.0, 'collect': 0.0}
         self.round_s = []
+        # per round: (wall s, device s of the batched steps, sessions due, cell updates, tunnels
+        # that joined, tunnels still being built, sessions retired before it, issue s, collect s)
+        self.round_log = []
         self.step_gpu_s = 0.0  # device time of the batched steps (CUDA events on the batch stream)
         self.step_cells = 0
 
@@ -339,11 +344,12 @@ class SessionServer:
 
     def _frame_steps(self, s):
         """Steps before a session's next frame: none while paused; its own 'steps' with the
-        streams executor (each tunnel its own launch); the server's steps_per_frame with the
-        persistent one (one launch steps every tunnel alike)."""
+        streams executor (each tunnel its own launch) and the parameter-space batched tiles
+        (200 + k, each step launching the tunnels with steps to go); the server's
+        steps_per_frame with the work-list forms (one launch steps every tunnel alike)."""
         if not s.running:
             return 0
-        if self.batch_mode == 'streams':
+        if self.steps_each:
             return int(s.p.get('steps', self.steps_per_frame))
         return self.steps_per_frame
 
@@ -472,8 +478,10 @@ class SessionServer:
             self.t0 = now
         self.round_frames = []  # (session id, frame bytes) of this round, for the sender
         self._apply_commands(now)
+        retired0, joined0 = self.retired, self.admitted
         self._retire(now)
         self._admit(now)
+        retired, joined = self.retired - retired0, self.admitted - joined0
         t_admit = self.clock()
         due = sorted((s for s in self.active.values() if self._due(s, now)), key=lambda s: s.request_t)
         self.max_active = max(self.max_active, len(self.active))
@@ -531,10 +539,15 @@ class SessionServer:
             if s.id in broken:
                 self._fail(s, broken[s.id])
         t_end = self.clock()
+        step_s, cells = 0.0, 0
         if started is not None:  # every frame has been collected, so both events are complete
             done.synchronize()
-            self.step_gpu_s += started.elapsed_time(done) / 1e3
-            self.step_cells += sum(s.n * ks[s.id] for s in stepping if s.id not in broken)
+            step_s = started.elapsed_time(done) / 1e3
+            cells = sum(s.n * ks[s.id] for s in stepping if s.id not in broken)
+            self.step_gpu_s += step_s
+            self.step_cells += cells
+        self.round_log.append((t_end - now, step_s, len(due), cells, joined, len(self.building), retired,
+                               t_issue - t_rebuild, t_end - t_issue))
         for name, a, b in (('admit', now, t_admit), ('rebuild', t_admit, t_rebuild), ('issue', t_rebuild, t_issue),
                            ('collect', t_issue, t_end)):
             self.phase[name] += b - a
@@ -595,12 +608,34 @@ class SessionServer:
                              **{f'{k}_mean': round(v / max(1, self.rounds) * 1e3, 2) for k, v in self.phase.items()}},
                 'frames_per_session_s': round(len(self.latencies) / span / max(1e-9, self.active_sum / max(1, self.rounds)), 2),
                 'requested_glups_end': round(self.demand / 1e9, 2),
-                'work_bound_glups': None if self.work_bound is None else round(self.work_bound / 1e9, 2)}
+                'work_bound_glups': None if self.work_bound is None else round(self.work_bound / 1e9, 2),
+                'slow_rounds': self.slow_rounds()}
+
+    def slow_rounds(self, k=8):
+        """The k longest rounds of the window beside the median one: wall and device step time,
+        sessions, cell updates and the device rate, tunnels that joined, tunnels still being
+        built, sessions retired just before, and the host's issue and collect phases."""
+        if not self.round_log:
+            return []
+        keys = ('ms', 'step_ms', 'sessions', 'gcells', 'joined', 'building', 'retired', 'issue_ms', 'collect_ms')
+        order = sorted(range(len(self.round_log)), key=lambda i: self.round_log[i][0])
+        pick = order[::-1][:k] + [order[len(order) // 2]]
+        out = []
+        for i in pick:
+            r = self.round_log[i]
+            d = dict(zip(keys, (round(r[0] * 1e3, 1), round(r[1] * 1e3, 1), r[2], round(r[3] / 1e9, 3), r[4], r[5],
+                                r[6], round(r[7] * 1e3, 1), round(r[8] * 1e3, 1))))
+            d['glups'] = round(r[3] / r[1] / 1e9, 2) if r[1] > 0 else None
+            d['round'] = i
+            out.append(d)
+        out[-1]['median'] = True
+        return out
 
     def reset_window(self):
         """Start a fresh measurement window (drop latencies and counters so far)."""
         self.latencies.clear()
         self.round_s.clear()
+        self.round_log.clear()
         self.phase = dict.fromkeys(self.phase, 0.0)
         self.step_gpu_s = 0.0
         self.step_cells = 0
@@ -673,7 +708,8 @@ class Arrivals:
 
 def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='fp32', seed=5, device='cuda:0',
              particles=5000, warm_start=True, tile=0, steps_per_frame=10, fps=30.0, mask_set=None, keep=None,
-             before_window=None, latencies_out=None, server_factory=None, warmup_s=0.0, work_bound_glups=None):
+             before_window=None, latencies_out=None, server_factory=None, warmup_s=0.0, work_bound_glups=None,
+             batch_mode='streams'):
     """Config 5 in wall-clock time: Poisson arrivals at `rate` per second for `duration`
     seconds, each session requesting `fps` frames per second of its particles, one slice and
     Cd/Cl, admitted against `budget` bytes. With warm_start the run begins from the arrival
@@ -691,7 +727,7 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     gen = Arrivals(seed, mean_life, particles, mask_set)
     srv = (server_factory or SessionServer)(device, budget_bytes=budget, precision=precision, fps=fps,
                                             steps_per_frame=steps_per_frame, tile=tile, admit_thread=True,
-                                            work_bound_glups=work_bound_glups)
+                                            work_bound_glups=work_bound_glups, batch_mode=batch_mode)
 
     def offer(s, t):
         if keep is None or keep(s, t):
@@ -736,7 +772,8 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     out = srv.stats()
     out.update(precision=precision, duration_s=duration, arrival_rate=rate, mean_lifetime_s=mean_life,
                budget_gb=budget / 1e9, warm_start=warm_start, steps_per_frame=steps_per_frame, fps=fps,
-               particles=particles, setup_s=round(setup_s, 1), warmup_s=warmup_s)
+               particles=particles, setup_s=round(setup_s, 1), warmup_s=warmup_s, batch_mode=batch_mode,
+               tile=srv.tile if batch_mode != 'streams' else None)
     if latencies_out is not None:
         latencies_out.extend(srv.latencies)
     srv.close()
@@ -754,12 +791,16 @@ def main(argv=None):
     ap.add_argument('--tile', type=int, default=0)
     ap.add_argument('--seed', type=int, default=5)
     ap.add_argument('--warmup', type=float, default=3.0, help='untimed seconds of rounds before the window')
+    ap.add_argument('--batch-mode', nargs='+', default=['streams'], choices=['streams', 'persistent'])
+    ap.add_argument('--work-bound', type=float, default=None, help='admission bound on requested GLUPS')
     a = ap.parse_args(argv)
     ms = masks()
     for prec in a.precision:
-        r = simulate(a.duration, a.rate, a.mean_life, a.budget_gb * 1e9, prec, a.seed, tile=a.tile,
-                     steps_per_frame=a.steps_per_frame, mask_set=ms, warmup_s=a.warmup)
-        print(json.dumps(r), flush=True)
+        for mode in a.batch_mode:
+            r = simulate(a.duration, a.rate, a.mean_life, a.budget_gb * 1e9, prec, a.seed, tile=a.tile,
+                         steps_per_frame=a.steps_per_frame, mask_set=ms, warmup_s=a.warmup, batch_mode=mode,
+                         work_bound_glups=a.work_bound)
+            print(json.dumps(r), flush=True)
 
 
 if __name__ == '__main__':

@@ -23,7 +23,7 @@ EXPORTS = ['wt_last_error', 'wt_abi_version', 'wt_check_dims', 'wt_population_by
            'wt_build_codes', 'wt_links_scratch_len', 'wt_links_scan', 'wt_links_fill', 'wt_step_tiles', 'wt_step',
            'wt_step_test_skip_chunk',
            'wt_reduce_scratch_len', 'wt_forces', 'wt_forces_noalloc', 'wt_mass', 'wt_batch_workspace_bytes',
-           'wt_batch_create', 'wt_batch_step', 'wt_batch_capture', 'wt_batch_replay', 'wt_batch_cur',
+           'wt_batch_create', 'wt_batch_step', 'wt_batch_step_each', 'wt_batch_capture', 'wt_batch_replay', 'wt_batch_cur',
            'wt_batch_destroy', 'wt_advect', 'wt_pack_particles', 'wt_slice', 'wt_cp',
            'wt_voxelize_workspace_bytes', 'wt_voxelize']
 
@@ -45,7 +45,7 @@ class Grid(ctypes.Structure):
 
 
 _lib = None
-ABI_VERSION = 3  # include/wt.h WT_ABI_VERSION this binding is written against
+ABI_VERSION = 4  # include/wt.h WT_ABI_VERSION this binding is written against
 
 
 def lib():
@@ -77,6 +77,7 @@ def lib():
             'wt_batch_workspace_bytes': ([gp, i32, i32], i64),
             'wt_batch_create': ([gp, i32, vp, vp, vp, vp, i32, vp, i64, vp, ctypes.POINTER(vp)], ctypes.c_int),
             'wt_batch_step': ([vp, i32, i32, vp], ctypes.c_int),
+            'wt_batch_step_each': ([vp, vp, i32, vp], ctypes.c_int),
             'wt_batch_capture': ([vp, i32, i32, vp], ctypes.c_int),
             'wt_batch_replay': ([vp, vp], ctypes.c_int),
             'wt_batch_cur': ([vp, vp], ctypes.c_int),
