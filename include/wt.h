@@ -162,9 +162,9 @@ int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void*
  * 103, 104, 118) as one block per work-list tile; 200 + k (203, 204, 218, and 229, which is
  * tile 18 with each pair's pull issued with its code bytes) with the tunnels' descriptors in
  * the kernel parameters, one block per tile of BLOCK * V cells, groups of tunnels that fit the
- * 32 KB parameter space per launch, and no device work list; 0 = default. The caller allocates
+ * 32 KB parameter space per launch, and no device work list. The caller allocates
  * a 256-byte aligned device workspace of wt_batch_workspace_bytes (descriptor table and work
- * lists; 256 bytes, unused, for the 200 + k forms). cur gives each tunnel's
+ * lists; 256 bytes, unused, for the 200 + k forms). Tile 0 is 229 (204 for fp64). cur gives each tunnel's
  * current population buffer at creation; wt_batch_cur reports it later. A batch must be
  * re-created after any of its tunnels is stepped on its own. */
 typedef struct wt_batch wt_batch;

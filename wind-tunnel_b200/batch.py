@@ -61,7 +61,8 @@ class TunnelBatch:
         self._smag = dbl(*[float(p['smag']) for p in params])
         self._cur = (ctypes.c_int32 * n)(*[s.cur for s in self.solvers])
         self.tile = int(tile)
-        self.steps_each = self.tile // 100 == 2  # per-tunnel step counts in one batch
+        # per-tunnel step counts in one batch: the parameter-space tiles (tile 0 is one of them)
+        self.steps_each = self.tile == 0 or self.tile // 100 == 2
         self.params = [dict(p) for p in params]
         self.cells = sum(s.n for s in self.solvers)
         self.handle = ctypes.c_void_p()
