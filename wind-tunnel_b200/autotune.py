@@ -101,3 +101,68 @@ def tune(solver, params, steps=8, warm=2, repeats=2, force=False):
     _cache[_key(solver)] = {'tile': tid, 'ms': timings}
     _save_file()
     return tid, timings
+
+
+def compare(solver, params, tiles, steps=50, repeats=5, developed=1000):
+    """Median ms per step of each tile in `tiles`, timed in interleaved repeats (tile order
+    inside each repeat) so that clock and power drift fall alike on every tile: first right
+    after the caller's reset ('fresh'), then after `developed` more steps with the first tile
+    ('developed'). Returns {'fresh': {tile: ms}, 'developed': {tile: ms}}."""
+    import statistics
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    out = {}
+    for phase in ('fresh', 'developed'):
+        if phase == 'developed':
+            solver.set_tile(tiles[0])
+            solver.step(developed, params)
+        reps = {t: [] for t in tiles}
+        for _ in range(repeats):
+            for t in tiles:
+                solver.set_tile(t)
+                solver.step(2, params)
+                ev0.record(solver.stream)
+                solver.step(steps, params)
+                ev1.record(solver.stream)
+                ev1.synchronize()
+                reps[t].append(ev0.elapsed_time(ev1) / steps)
+        out[phase] = {t: statistics.median(v) for t, v in reps.items()}
+    return out
+
+
+def main(argv=None):
+    """python wind-tunnel_b200/autotune.py [--scale S] FORM:TILE,TILE ... -- compare tiles of each
+    storage form (e.g. fp16-fast:21,31) on the benchmark body, fresh and developed."""
+    import argparse
+    import bodies
+    import lbm
+    ap = argparse.ArgumentParser(description='compare step tiles on the benchmark body')
+    ap.add_argument('forms', nargs='+', help='precision-collision:tile,tile,...')
+    ap.add_argument('--scale', type=float, default=1.0, help='grid scale (1.0 = 512x256x256)')
+    ap.add_argument('--steps', type=int, default=50)
+    ap.add_argument('--repeats', type=int, default=5)
+    ap.add_argument('--developed', type=int, default=1000)
+    a = ap.parse_args(argv)
+    dims, solid, p = bodies.config2(scale=a.scale)
+    n = dims[0] * dims[1] * dims[2]
+    result = {}
+    for spec in a.forms:
+        form, tl = spec.split(':')
+        prec, coll = form.split('-')
+        tiles = [int(t) for t in tl.split(',')]
+        s = lbm.Solver(dims, 'cuda:0', precision=prec, collision=coll)
+        s.set_solid(solid)
+        s.reset(p['uIn'])
+        r = compare(s, p, tiles, a.steps, a.repeats, a.developed)
+        for phase, ms in r.items():
+            for t, v in ms.items():
+                print(f'{form} {phase} tile {t}: {v:.4f} ms {n / v / 1e6:.2f} GLUPS', flush=True)
+        result[form] = {ph: {str(t): round(v, 4) for t, v in ms.items()} for ph, ms in r.items()}
+        del s
+        torch.cuda.empty_cache()
+    print(json.dumps({'dims': list(dims), 'steps': a.steps, 'repeats': a.repeats, 'developed': a.developed,
+                      'ms_per_step': result}))
+
+
+if __name__ == '__main__':
+    main()

@@ -68,7 +68,8 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
 // grid with the face cells of k_step_faces computed by the blocks of the rows they read
 // (k_step_rows with FUSE), so the step is one kernel. Tiles 29-32 issue each pair's pull
 // together with its code bytes instead of after them (EARLY): 29 is tile 18 so, 30-32 are
-// tiles 19, 21 and 22. wt_grid.tile
+// tiles 19, 21 and 22, and 33-35 the same rows at 32 threads x 32 blocks and 64 threads x 14
+// or 12 blocks per SM. wt_grid.tile
 // selects one (0 = the default for the precision and collision form); autotune.py times them.
 #define WT_VARIANTS(PREC, FAST)                                                          \
     {1, 0, 1, 256, 4, 0, 0, launch_bulk<PREC, FAST, 1, 256, 4>},                         \
@@ -102,7 +103,10 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     {29, 0, 2, 128, 8, 0, 0, launch_bulk<PREC, FAST, 2, 128, 8, true>},                  \
     {30, 2, 2, 128, 8, 0, 0, launch_rows<PREC, FAST, 128, 8, 0, false, true>},           \
     {31, 2, 2, 64, 16, 0, 0, launch_rows<PREC, FAST, 64, 16, 0, false, true>},           \
-    {32, 2, 2, 64, 16, 0, 1, launch_rows<PREC, FAST, 64, 16, 1, false, true>}
+    {32, 2, 2, 64, 16, 0, 1, launch_rows<PREC, FAST, 64, 16, 1, false, true>},           \
+    {33, 2, 2, 32, 32, 0, 0, launch_rows<PREC, FAST, 32, 32, 0, false, true>},           \
+    {34, 2, 2, 64, 14, 0, 0, launch_rows<PREC, FAST, 64, 14, 0, false, true>},           \
+    {35, 2, 2, 64, 12, 0, 0, launch_rows<PREC, FAST, 64, 12, 0, false, true>}
 
 template <int PREC, bool FAST>
 const StepVariant* variants_of(int* count) {
