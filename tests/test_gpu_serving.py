@@ -179,3 +179,46 @@ def test_client_commands_match_the_engine_semantics(mode, tile):
         assert len(got[s0.id]) == rounds
         for r, (a, b) in enumerate(zip(got[s0.id], want)):
             assert a == b, f'session {s0.id} frame {r}'
+
+
+@pytest.mark.parametrize('precision', ['fp32', 'fp16'])
+def test_recycled_tunnel_equals_a_new_one(precision):
+    """A Solver that served one session (surface, particles, frames with Cp, an odd step count)
+    and is then recycled gives the next session the frames and populations a new Solver gives."""
+    import bodies
+    import serving
+    from lbm import Solver
+    dims = (64, 24, 20)
+    first = _sessions()[0]
+    second = serving.Session(7, dims, bodies.ellipsoid_union(dims, 3, 977, scale=dims[0] / 256.0, floor='belt')[0],
+                             dict(uIn=0.06, tau=0.52, smag=0.16), 1e9, particles=150)
+    verts, norms = bodies.surface_points(first.solid, dims)
+
+    def frames(sv, s, n, k, cp):
+        out = []
+        for _ in range(n):
+            sv.step(k, s.p)
+            sv.advance_particles(k, s.p)
+            sv.launch_frame_packed(s.p, cp)
+            header = dict(type='frame', dims=list(dims), numP=sv.num_p, numVerts=sv.num_verts, forces=None, steps=k,
+                          mlups=0.0, running=True)
+            out.append(sv.collect_frame_packed(header))
+        return out
+
+    used = Solver(dims, 'cuda:0', precision=precision, seed=first.id)
+    used.set_solid(first.solid)
+    used.set_surface(verts, norms)
+    used.reset(first.p['uIn'])
+    used.set_particles(first.particles, first.p)
+    frames(used, first, 3, 7, True)
+    used.recycle(seed=second.id)
+    fresh = Solver(dims, 'cuda:0', precision=precision, seed=second.id)
+    got = {}
+    for name, sv in (('recycled', used), ('new', fresh)):
+        sv.set_solid(second.solid)
+        sv.reset(second.p['uIn'])
+        sv.set_particles(second.particles, second.p)
+        got[name] = (frames(sv, second, 4, 10, False), sv.populations(), sv.macro())
+    assert got['recycled'][0] == got['new'][0]
+    assert np.array_equal(got['recycled'][1], got['new'][1])
+    assert np.array_equal(got['recycled'][2], got['new'][2])

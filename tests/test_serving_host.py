@@ -88,10 +88,10 @@ class FakeBatch:
         self.closed = True
 
 
-def _server(clock, rate=1e12, budget=100.0, **kw):
+def _server(clock, rate=1e12, budget=100.0, solver_factory=FakeSolver, **kw):
     FakeBatch.log = []
     FakeBatch.steps = []
-    return serving.SessionServer(device=None, budget_bytes=budget, clock=clock, solver_factory=FakeSolver,
+    return serving.SessionServer(device=None, budget_bytes=budget, clock=clock, solver_factory=solver_factory,
                                  batch_factory=lambda sv, p: FakeBatch(clock, rate, sv),
                                  footprint=lambda s: float(s.n), **kw)
 
@@ -469,3 +469,63 @@ def test_admission_worker_builds_tunnels_while_rounds_run():
     finally:
         gate.set()
         srv.close()
+
+
+class RecyclingSolver(FakeSolver):
+    made = 0
+
+    def __init__(self, s):
+        super().__init__(s)
+        RecyclingSolver.made += 1
+        self.recycled = 0
+
+    def recycle(self, seed=None):
+        self.recycled += 1
+
+
+def _recycling_factory(s):
+    sv = s.reuse
+    if sv is None:
+        return RecyclingSolver(s)
+    s.reuse = None
+    sv.recycle(s.id)
+    sv.s = s
+    return sv
+
+
+def test_retired_tunnels_are_kept_and_reused_by_the_same_grid():
+    c = Clock()
+    RecyclingSolver.made = 0
+    srv = _server(c, budget=20, solver_factory=_recycling_factory)
+    a, b = _session(0, 6, life=1.0), _session(1, 4, life=1.0)
+    srv.submit(a)
+    srv.submit(b)
+    srv.round()
+    c.t = 1.0  # both retire; their tunnels are kept, still charged to the budget
+    srv.round()
+    assert srv.retired == 2 and srv.used == 0 and srv.pooled == 10 and a.solver is None
+    d = _session(2, 6)  # the grid of session 0: takes its tunnel, no new solver
+    srv.submit(d)
+    srv.round()
+    assert srv.pool_hits == 1 and RecyclingSolver.made == 2 and d.solver.recycled == 1
+    assert srv.used == 6 and srv.pooled == 4
+    e = _session(3, 12)  # another grid that needs the kept 4 bytes: the kept tunnel is dropped
+    srv.submit(e)
+    srv.round()
+    assert srv.pool_evictions == 1 and srv.pooled == 0 and srv.used == 18 and RecyclingSolver.made == 3
+    st = srv.stats()
+    assert st['tunnels_reused'] == 1 and st['kept_tunnels_dropped'] == 1 and st['kept_gb_end'] == 0
+
+
+def test_a_kept_tunnel_waits_when_memory_is_short_and_is_never_dropped_for_its_own_grid():
+    c = Clock()
+    srv = _server(c, budget=10, solver_factory=_recycling_factory)
+    srv.submit(_session(0, 6, life=1.0))
+    srv.submit(_session(1, 4))
+    srv.round()
+    c.t = 1.0
+    srv.round()
+    assert srv.pooled == 6 and srv.used == 4
+    srv.submit(_session(2, 6))  # its grid's tunnel is kept: 4 + 6 fits exactly
+    srv.round()
+    assert srv.pool_hits == 1 and srv.pool_evictions == 0 and srv.used == 10 and srv.pooled == 0

@@ -137,6 +137,30 @@ class Solver:
         self._pending = None
         self.stream.synchronize()
 
+    def recycle(self, seed=None):
+        """Return to the state right after construction with ``seed``, keeping the device and
+        pinned buffers: a new tunnel of the same grid, precision and collision form (a serving
+        session replacing one that left) then needs no allocation, which would hold driver and
+        interpreter locks while other tunnels are being launched. Populations, macros, mask and
+        codes are zeroed, and links, particles, surface, tile and pending frames are dropped,
+        as a new Solver has them."""
+        self.synchronize()
+        with torch.cuda.stream(self.stream):
+            for t in (*self.f, *self.mac, self.solid, self.code, self.status_dev):
+                t.zero_()
+        self.n_links = 0
+        self.grid.tile = 0
+        self.grid.shift_u = 0.0
+        self.cur = 0
+        self.num_p = 0
+        self.num_verts = 0
+        self.seed = 1
+        self.rng = np.random.default_rng(seed)
+        self._pending = None
+        self._pk_pending = None
+        self._pk_layout_key = None  # the next layout zeroes the packed-frame buffer
+        self.stream.synchronize()
+
     def set_tile(self, tile):
         """Select a step-kernel tile variant (see wtlib.step_tiles; 0 = library default)."""
         self.grid.tile = int(tile)
@@ -163,9 +187,11 @@ class Solver:
         codes and the compacted momentum-exchange link list."""
         arr = np.asarray(arr)
         assert arr.size == self.n
-        host = torch.from_numpy(np.ascontiguousarray(arr.reshape(-1).astype(np.uint8)))
+        # no copy of a mask that is already contiguous uint8, no second staging of pinned memory
+        a = np.ascontiguousarray(arr.reshape(-1), dtype=np.uint8)
+        host = torch.from_numpy(a if a.flags.writeable else a.copy())  # uploads are read-only views
         with torch.cuda.stream(self.stream):
-            self.solid.copy_(host.pin_memory(), non_blocking=True)
+            self.solid.copy_(host if host.is_pinned() else host.pin_memory(), non_blocking=True)
             call('wt_build_codes', self.gp, self.sh)
             scratch = torch.empty(int(W.lib().wt_links_scratch_len(self.n)), dtype=torch.int64, device=self.dev)
             count = torch.zeros(1, dtype=torch.int64, device=self.dev)

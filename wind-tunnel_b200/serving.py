@@ -77,6 +77,7 @@ class Session:
         self.arrival = float(arrival)
         self.frontal = frontal if frontal is not None else bodies.areas(solid, self.dims)[0]
         self.solver = None
+        self.reuse = None          # a kept tunnel of this grid, re-initialised for this session
         self.bytes = 0
         self.request_t = None
         self.admitted_t = None
@@ -109,7 +110,7 @@ class SessionServer:
     def __init__(self, device='cuda:0', budget_bytes=160e9, precision='fp32', fps=30.0, steps_per_frame=10,
                  tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
                  footprint=None, keep_frames=False, batch_mode='streams', pacing='fps', paused_hz=PAUSED_HZ,
-                 rate_in_header=True, priorities=True, work_bound_glups=None, admit_thread=False):
+                 rate_in_header=True, priorities=True, work_bound_glups=None, admit_thread=False, recycle=True):
         self.device = device
         self.budget = float(budget_bytes)
         self.precision = precision
@@ -127,6 +128,10 @@ class SessionServer:
         self.steps_each = batch_mode == 'streams' or self.tile // 100 == 2
         self.clock = clock
         self.solver_factory = solver_factory or self._make_solver
+        # the default factory's tunnels are allocated on the serving thread at admission, when
+        # the GPU is idle between rounds (an allocator that frees its cache synchronises the
+        # device, and allocation holds driver locks), and initialised on the worker thread
+        self._allocate = self._alloc_solver if solver_factory is None else None
         self.batch_factory = batch_factory or self._make_batch
         self.footprint = footprint or (lambda s: lbm.estimate_bytes(s.dims, precision, s.particles))
         self.keep_frames = keep_frames
@@ -146,10 +151,19 @@ class SessionServer:
         # fps) stay within work_bound_glups; None admits by the HBM budget alone
         self.work_bound = None if work_bound_glups is None else float(work_bound_glups) * 1e9
         self.demand = 0.0
-        # admit_thread: a worker thread builds admitted sessions' tunnels (allocation, mask
-        # upload, link list, particles, pinned frame buffers) while rounds run; a session joins
-        # the first round after its tunnel is ready, and commands sent meanwhile wait for it.
-        # Without it (the default) admission builds the tunnel inside the round.
+        # admit_thread: a worker thread initialises admitted sessions' tunnels (mask upload,
+        # codes, link list, equilibrium, particles) while rounds run, after admission has
+        # allocated them or taken kept ones; a session joins the first round after its tunnel
+        # is ready, and commands sent meanwhile wait for it. Without it (the default) admission
+        # builds the tunnel inside the round.
+        # recycle: a retired session's tunnel (when its solver has recycle()) is kept, its bytes
+        # still charged to the budget, for the next session of the same grid, precision and
+        # collision form, which re-initialises it instead of allocating; admission evicts kept
+        # tunnels of other grids when it needs their memory
+        self.recycle = recycle
+        self._pool = {}                     # (dims, particles) -> [(solver, bytes)] kept tunnels
+        self.pooled = 0.0
+        self.pool_hits = self.pool_evictions = 0
         self.building = {}                  # id -> Session whose tunnel the worker is building
         self._built = collections.deque()   # (session, exception or None) the worker finished
         self._jobs = None
@@ -214,11 +228,25 @@ class SessionServer:
             return 0
         return -3 if s.n <= 1_000_000 else (-2 if s.n <= 4_000_000 else (-1 if s.n <= 16_000_000 else 0))
 
-    def _make_solver(self, s):
+    def _alloc_solver(self, s):
+        """A new tunnel's device and pinned frame buffers (lbm.Solver), on its own stream."""
         import torch
         stream = torch.cuda.Stream(torch.device(self.device), priority=self._priority(s))
         sv = lbm.Solver(s.dims, self.device, precision=self.precision, collision=self.collision, seed=s.id,
                         stream=stream)
+        sv.prepare_frame(s.p, s.verts is not None)
+        sv.fresh = True
+        return sv
+
+    def _make_solver(self, s):
+        if s.reuse is not None:  # a kept tunnel of this grid, or one allocated at admission
+            sv, s.reuse = s.reuse, None
+            if not getattr(sv, 'fresh', False):
+                sv.recycle(seed=s.id)
+            sv.fresh = False
+        else:
+            sv = self._alloc_solver(s)
+            sv.fresh = False
         sv.set_solid(s.solid)
         sv.reset(s.p['uIn'])
         if s.particles:
@@ -395,7 +423,7 @@ class SessionServer:
             self.used -= s.bytes
             self._activate(s, now)
             self.used += s.bytes
-            self.peak_used = max(self.peak_used, self.used)
+            self.peak_used = max(self.peak_used, self.used + self.pooled)
             for msg, payload in s.deferred:  # commands sent while it was being built
                 self._apply_one(s, msg, payload, now)
             s.deferred = []
@@ -406,18 +434,38 @@ class SessionServer:
                 self.abandoned += 1
                 continue
             need = self.footprint(s)
-            if self.used + need > self.budget:
-                break
+            key = self._pool_key(s)
+            kept = self._pool.get(key)
+            reuse_bytes = kept[-1][1] if kept else 0.0
+            over = self.used + self.pooled - reuse_bytes + max(need, reuse_bytes) - self.budget
+            if over > 0:  # drop kept tunnels, never the one this session would take
+                self._evict(over, spare=key if kept else None)
+                if self.used + self.pooled - reuse_bytes + max(need, reuse_bytes) > self.budget:
+                    break
             want = self._demand(s)
             if self.work_bound is not None and self.active and self.demand + want > self.work_bound:
                 break
             self.queue.pop(0)
+            if kept:  # the kept tunnel of this grid leaves the pool for this session
+                s.reuse, b = kept.pop()
+                if not kept:
+                    del self._pool[key]
+                self.pooled -= b
+                need = max(need, b)
+                self.pool_hits += 1
             s.demand = want
             if self._jobs is not None:  # built by the worker; memory and demand reserved now
+                if s.reuse is None and self._allocate is not None:
+                    try:
+                        s.reuse = self._allocate(s)
+                    except Exception as e:  # out of memory etc. (server/app.py:115-122)
+                        self.failed += 1
+                        self.errors.append((s.id, f'Could not allocate {"x".join(map(str, s.dims))} grid: {e}'))
+                        continue
                 s.bytes = need
                 self.used += need
                 self.demand += want
-                self.peak_used = max(self.peak_used, self.used)
+                self.peak_used = max(self.peak_used, self.used + self.pooled)
                 self.building[s.id] = s
                 self._jobs.put(s)
                 continue
@@ -432,7 +480,7 @@ class SessionServer:
             self._activate(s, now)
             self.demand += want
             self.used += s.bytes
-            self.peak_used = max(self.peak_used, self.used)
+            self.peak_used = max(self.peak_used, self.used + self.pooled)
         self.max_active = max(self.max_active, len(self.active))
 
     def _demand(self, s):
@@ -466,8 +514,33 @@ class SessionServer:
             self.used -= s.bytes
             self.demand -= getattr(s, 'demand', 0.0)
             s.solver.synchronize()
+            if self.recycle and hasattr(s.solver, 'recycle'):
+                self._pool.setdefault(self._pool_key(s), []).append((s.solver, s.bytes))
+                self.pooled += s.bytes
             s.solver = None
             self.retired += 1
+
+    def _pool_key(self, s):
+        return tuple(s.dims)  # precision and collision form are the server's
+
+    def _evict(self, need, spare=None):
+        """Drop kept tunnels, the largest first, until `need` bytes are free; the last kept
+        tunnel of grid `spare` (the one an arriving session takes) stays."""
+        order = sorted(((k, j) for k, v in self._pool.items() for j in range(len(v))
+                        if not (k == spare and j == len(v) - 1)),
+                       key=lambda kj: -self._pool[kj[0]][kj[1]][1])
+        drop = []
+        for k, j in order:
+            if need <= 0:
+                break
+            need -= self._pool[k][j][1]
+            drop.append((k, j))
+        for k, j in sorted(drop, key=lambda kj: -kj[1]):
+            _, b = self._pool[k].pop(j)
+            self.pooled -= b
+            self.pool_evictions += 1
+            if not self._pool[k]:
+                del self._pool[k]
 
     # ---- one round ----
     def round(self):
@@ -600,6 +673,8 @@ class SessionServer:
                 'max_active': self.max_active,
                 'mean_active': round(self.active_sum / max(1, self.rounds), 1), 'queued_end': len(self.queue),
                 'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
+                'kept_gb_end': round(self.pooled / 1e9, 2), 'tunnels_reused': self.pool_hits,
+                'kept_tunnels_dropped': self.pool_evictions,
                 'peak_used_gb': round(self.peak_used / 1e9, 2),
                 'glups': round(self.cell_updates / span / 1e9, 3),
                 'step_glups_device': round(self.step_cells / max(1e-9, self.step_gpu_s) / 1e9, 3),
@@ -659,6 +734,8 @@ class SessionServer:
         for s in self.active.values():
             s.solver.synchronize()
         self.active.clear()
+        self._pool.clear()
+        self.pooled = 0.0
 
 
 # ---- config 5: Poisson arrivals of tunnels of four sizes ----
