@@ -529,3 +529,22 @@ def test_a_kept_tunnel_waits_when_memory_is_short_and_is_never_dropped_for_its_o
     srv.submit(_session(2, 6))  # its grid's tunnel is kept: 4 + 6 fits exactly
     srv.round()
     assert srv.pool_hits == 1 and srv.pool_evictions == 0 and srv.used == 10 and srv.pooled == 0
+
+
+def test_at_most_new_per_round_tunnels_are_allocated_each_round():
+    c = Clock()
+    RecyclingSolver.made = 0
+    srv = _server(c, budget=100, solver_factory=_recycling_factory, new_per_round=1)
+    srv.submit(_session(0, 4, life=1.0))
+    srv.round()
+    c.t = 1.0
+    srv.round()  # session 0 retires; its tunnel is kept
+    for i in (1, 2, 3):
+        srv.submit(_session(i, 5 if i != 2 else 4))
+    c.t = 1.1
+    srv.round()  # 1 is this round's allocation; 2 takes the kept tunnel (not counted); 3 waits
+    assert list(srv.active) == [1, 2] and [s.id for s in srv.queue] == [3]
+    assert RecyclingSolver.made == 2 and srv.pool_hits == 1
+    c.t = 1.2
+    srv.round()  # the next round allocates 3
+    assert list(srv.active) == [1, 2, 3] and RecyclingSolver.made == 3

@@ -173,6 +173,7 @@ def make_app(srv, gpu_name='CUDA device', memory=None):
 
 
 def main(argv=None):
+    serving.expandable_segments()
     ap = argparse.ArgumentParser(description='WebSocket front end of the wind-tunnel sessions on one GPU')
     ap.add_argument('--port', type=int, default=8765)
     ap.add_argument('--host', default='0.0.0.0')
@@ -182,7 +183,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     import torch
     srv = serving.SessionServer(a.device, budget_bytes=a.budget_gb * 1e9, precision=a.precision, pacing='client',
-                                admit_thread=True)
+                                admit_thread=True, new_per_round=1)
     name = torch.cuda.get_device_name(torch.device(a.device))
     web.run_app(make_app(srv, name, int(a.budget_gb * 1e9)), host=a.host, port=a.port, print=None)
 

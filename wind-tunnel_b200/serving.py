@@ -45,6 +45,7 @@ import argparse
 import collections
 import heapq
 import json
+import os
 import time
 
 import numpy as np
@@ -110,7 +111,8 @@ class SessionServer:
     def __init__(self, device='cuda:0', budget_bytes=160e9, precision='fp32', fps=30.0, steps_per_frame=10,
                  tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
                  footprint=None, keep_frames=False, batch_mode='streams', pacing='fps', paused_hz=PAUSED_HZ,
-                 rate_in_header=True, priorities=True, work_bound_glups=None, admit_thread=False, recycle=True):
+                 rate_in_header=True, priorities=True, work_bound_glups=None, admit_thread=False, recycle=True,
+                 new_per_round=None):
         self.device = device
         self.budget = float(budget_bytes)
         self.precision = precision
@@ -161,6 +163,10 @@ class SessionServer:
         # collision form, which re-initialises it instead of allocating; admission evicts kept
         # tunnels of other grids when it needs their memory
         self.recycle = recycle
+        # new_per_round: at most this many tunnels are newly allocated per round (kept tunnels
+        # are not counted); allocating several large tunnels at once under a nearly full
+        # budget can take the allocator hundreds of milliseconds, all of it in one round
+        self.new_per_round = new_per_round
         self._pool = {}                     # (dims, particles) -> [(solver, bytes)] kept tunnels
         self.pooled = 0.0
         self.pool_hits = self.pool_evictions = 0
@@ -411,6 +417,7 @@ class SessionServer:
         self.admitted += 1
 
     def _admit(self, now):
+        allocated = 0
         while self._built:  # tunnels the worker finished join this round
             s, err = self._built.popleft()
             del self.building[s.id]
@@ -436,6 +443,8 @@ class SessionServer:
             need = self.footprint(s)
             key = self._pool_key(s)
             kept = self._pool.get(key)
+            if not kept and self.new_per_round is not None and allocated >= self.new_per_round:
+                break  # the next round allocates it
             reuse_bytes = kept[-1][1] if kept else 0.0
             over = self.used + self.pooled - reuse_bytes + max(need, reuse_bytes) - self.budget
             if over > 0:  # drop kept tunnels, never the one this session would take
@@ -454,6 +463,8 @@ class SessionServer:
                 need = max(need, b)
                 self.pool_hits += 1
             s.demand = want
+            if not kept:
+                allocated += 1
             if self._jobs is not None:  # built by the worker; memory and demand reserved now
                 if s.reuse is None and self._allocate is not None:
                     try:
@@ -804,7 +815,7 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     gen = Arrivals(seed, mean_life, particles, mask_set)
     srv = (server_factory or SessionServer)(device, budget_bytes=budget, precision=precision, fps=fps,
                                             steps_per_frame=steps_per_frame, tile=tile, admit_thread=True,
-                                            work_bound_glups=work_bound_glups, batch_mode=batch_mode)
+                                            work_bound_glups=work_bound_glups, batch_mode=batch_mode, new_per_round=1)
 
     def offer(s, t):
         if keep is None or keep(s, t):
@@ -857,7 +868,15 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     return out
 
 
+def expandable_segments():
+    """Let torch's allocator grow mapped segments instead of keeping separate blocks per size, so
+    memory that one tunnel size freed serves another without returning it to the driver (which
+    synchronises the device). Effective only before the process's first CUDA allocation."""
+    os.environ.setdefault('PYTORCH_CUDA_ALLOC_CONF', 'expandable_segments:True')
+
+
 def main(argv=None):
+    expandable_segments()
     ap = argparse.ArgumentParser(description='Config 5 serving simulation (Poisson sessions on one GPU)')
     ap.add_argument('--duration', type=float, default=300.0)
     ap.add_argument('--rate', type=float, default=2.0)
