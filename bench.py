@@ -20,8 +20,8 @@ tunnels never exchange data); time is the max over ranks.
 The line also carries, for the fp32 default run: `roofline` (the fused step alone against the
 HBM peak, with a 2 GiB device copy timed in the same run beside it), `cpu_baseline` (the
 oracle on the host cores), `precision_variants` (fp32 fast, fp16 and bf16 shifted storage,
-fp16 exact), `accuracy_vs_fp64` (a chaotic and a laminar regime against an fp64 run, and the
-chaotic regime's statistics over 40,000 steps),
+fp16 exact), `accuracy_vs_fp64` (a chaotic and a laminar regime against an fp64 run; with
+`--accuracy-long` also the chaotic regime's statistics over 40,000 steps),
 `batching` (the 24-tunnel batch of config 4 under both batch executors, every tunnel re-run
 alone and compared bit for bit), and `voxelize` (the server-side voxeliser on the benchmark
 body). At N = 1 it carries `serving`: the config-5 serving loop (Poisson sessions of
@@ -495,8 +495,8 @@ def main():
     ap.add_argument('--no-accuracy', dest='accuracy', action='store_false')
     ap.add_argument('--no-batch', dest='batch', action='store_false')
     ap.add_argument('--accuracy-steps', type=int, default=2000)
-    ap.add_argument('--no-accuracy-long', dest='accuracy_long', action='store_false',
-                    help='skip the 40,000-step statistics regime of the accuracy study')
+    ap.add_argument('--accuracy-long', action='store_true',
+                    help='add the 40,000-step statistics regime to the accuracy study')
     ap.add_argument('--serving', type=float, default=20.0,
                     help='seconds of the config-5 serving run per precision (0 = skip; N = 1 only)')
     args = ap.parse_args()

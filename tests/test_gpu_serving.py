@@ -44,7 +44,7 @@ def _alone(s, frames, precision, k):
     return out
 
 
-EXECUTORS = [('streams', 0), ('persistent', 2), ('persistent', 229)]
+EXECUTORS = [('streams', 0), ('persistent', 2), ('persistent', 229), ('persistent', 231)]
 
 
 @pytest.mark.parametrize('mode,tile', EXECUTORS)

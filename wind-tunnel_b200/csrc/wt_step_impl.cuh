@@ -1129,6 +1129,7 @@ struct RowArgs {
     StepArgs<S, T> a;
     int64_t loff[Q];  // bytes from fin + idx0 to the aligned pull pair of population i
     int64_t soff[Q];  // bytes from fout + idx0 to population i of the output
+    FastDiv druns;    // blocks per lattice row (the parameter-space batch's block index to row)
 };
 
 template <int PREC, bool FAST>
@@ -1278,13 +1279,14 @@ __device__ __forceinline__ void pair_load_rows(const RowArgs<typename Prec<PREC>
     });
 }
 
-template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false, bool EARLY = false>
-__global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
+// One block of the row grid: x-run bx of lattice row (y, z).
+template <int PREC, bool FAST, int BLOCK, int ADDR, bool FUSE, bool EARLY>
+__device__ __forceinline__ void row_tile(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T>& r,
+                                         int32_t bx, int32_t y, int32_t z) {
     using T = typename Prec<PREC>::T;
     const auto& a = r.a;
-    const int32_t y = (int32_t)blockIdx.y, z = (int32_t)blockIdx.z;
     const int32_t nx = a.nx, ny = a.ny, nz = a.nz;
-    const int32_t x0 = ((int32_t)blockIdx.x * BLOCK + (int32_t)threadIdx.x) * 2;
+    const int32_t x0 = (bx * BLOCK + (int32_t)threadIdx.x) * 2;
     const bool valid = x0 < nx;
     const int32_t idx0 = x0 + nx * (y + ny * z);
     if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {  // a face row (uniform over the block)
@@ -1330,6 +1332,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typenam
             }
         }
     }
+}
+
+template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false, bool EARLY = false>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_rows(const RowArgs<typename Prec<PREC>::S, typename Prec<PREC>::T> r) {
+    row_tile<PREC, FAST, BLOCK, ADDR, FUSE, EARLY>(r, (int32_t)blockIdx.x, (int32_t)blockIdx.y, (int32_t)blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------

@@ -173,7 +173,6 @@ def make_app(srv, gpu_name='CUDA device', memory=None):
 
 
 def main(argv=None):
-    serving.expandable_segments()
     ap = argparse.ArgumentParser(description='WebSocket front end of the wind-tunnel sessions on one GPU')
     ap.add_argument('--port', type=int, default=8765)
     ap.add_argument('--host', default='0.0.0.0')

@@ -45,7 +45,6 @@ import argparse
 import collections
 import heapq
 import json
-import os
 import time
 
 import numpy as np
@@ -119,10 +118,12 @@ class SessionServer:
         self.collision = collision
         self.period = 1.0 / fps
         self.steps_per_frame = int(steps_per_frame)
-        # batched tile of the library executor: the parameter-space form of the two-cell tile
-        # with early pulls (229; 204, at 128 registers, for fp64), the fastest batched shape on
-        # config 4, which also steps sessions by their own counts
-        self.tile = int(tile) if tile else (204 if precision == 'fp64' else 229)
+        # batched tile of the library executor: the parameter-space form (sessions step by their
+        # own counts) of the precision's fastest single-tunnel body: the row grid with early
+        # pulls for fp16 / bf16 with the moment-space collision (231), the two-cell tile with
+        # early pulls otherwise (229; at 128 registers, 204, for fp64)
+        half_fast = precision in ('fp16', 'bf16') and collision in (None, 'fast')
+        self.tile = int(tile) if tile else (204 if precision == 'fp64' else (231 if half_fast else 229))
         # executor of the round's steps: every tunnel's own kernel on its own stream, all at
         # once ('streams'), or the library's batched kernels ('persistent': two launches per
         # step for all sessions)
@@ -868,15 +869,7 @@ def simulate(duration=300.0, rate=2.0, mean_life=60.0, budget=160e9, precision='
     return out
 
 
-def expandable_segments():
-    """Let torch's allocator grow mapped segments instead of keeping separate blocks per size, so
-    memory that one tunnel size freed serves another without returning it to the driver (which
-    synchronises the device). Effective only before the process's first CUDA allocation."""
-    os.environ.setdefault('PYTORCH_CUDA_ALLOC_CONF', 'expandable_segments:True')
-
-
 def main(argv=None):
-    expandable_segments()
     ap = argparse.ArgumentParser(description='Config 5 serving simulation (Poisson sessions on one GPU)')
     ap.add_argument('--duration', type=float, default=300.0)
     ap.add_argument('--rate', type=float, default=2.0)
