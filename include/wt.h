@@ -159,14 +159,12 @@ int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void*
  * results are bit-identical to stepping it alone with wt_step. All tunnels share precision and
  * collision form. tile selects the shape: a direct-load tile id k of wt_step_tiles (1-5, 7, 18)
  * runs as a persistent kernel (one wave of blocks looping over the work list); 100 + k (102,
- * 103, 104, 118) as one block per work-list tile; 200 + k (203, 204, 218; 229, which is tile
- * 18 with each pair's pull issued with its code bytes; 231, the row grid of tile 31) with the
- * tunnels' descriptors in the kernel parameters, one block per tile of BLOCK * V cells (one
- * x-run of a lattice row for 231), groups of tunnels that fit the 32 KB parameter space per
- * launch, and no device work list. The caller allocates
+ * 103, 104, 118) as one block per work-list tile; 200 + k (203, 204, 218, and 229, which is
+ * tile 18 with each pair's pull issued with its code bytes) with the tunnels' descriptors in the
+ * kernel parameters, one block per tile of BLOCK * V cells, groups of tunnels that fit the 32 KB
+ * parameter space per launch, and no device work list. The caller allocates
  * a 256-byte aligned device workspace of wt_batch_workspace_bytes (descriptor table and work
- * lists; 256 bytes, unused, for the 200 + k forms). Tile 0 is 231 (the row grid of wt_step tile
- * 31) for fp16/bf16 with WT_COLLIDE_FAST, 204 for fp64, and 229 otherwise. cur gives each tunnel's
+ * lists; 256 bytes, unused, for the 200 + k forms). Tile 0 is 229 (204 for fp64). cur gives each tunnel's
  * current population buffer at creation; wt_batch_cur reports it later. A batch must be
  * re-created after any of its tunnels is stepped on its own. */
 typedef struct wt_batch wt_batch;

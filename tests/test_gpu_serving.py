@@ -44,7 +44,7 @@ def _alone(s, frames, precision, k):
     return out
 
 
-EXECUTORS = [('streams', 0), ('persistent', 2), ('persistent', 229), ('persistent', 231)]
+EXECUTORS = [('streams', 0), ('persistent', 2), ('persistent', 229)]
 
 
 @pytest.mark.parametrize('mode,tile', EXECUTORS)

@@ -63,16 +63,13 @@ size_t desc_bytes_for(int32_t precision) {
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 // tile shape of a batch (direct-load variants only; 100 + k is the grid form of tile k, 200 + k
-// its parameter-space form); 0 picks the parameter-space form of the precision's single-tunnel
-// default: the row grid with early pulls (231) for fp16 / bf16 with the moment-space collision,
-// the two-cell tile with early pulls (229) otherwise, at 128 registers (204) for fp64
-int tile_shape(int32_t tile, int32_t precision, int32_t collision, int* v, int* block) {
+// its parameter-space form); 0 picks the parameter-space two-cell tile with early pulls (229),
+// or at 128 registers (204) for fp64
+int tile_shape(int32_t tile, int32_t precision, int* v, int* block) {
     static const int ids[][3] = {{1, 1, 256},   {2, 1, 128},   {3, 2, 128},   {4, 2, 128},   {5, 4, 128},
                                  {7, 2, 256},   {18, 2, 128},  {102, 1, 128}, {103, 2, 128}, {104, 2, 128},
-                                 {118, 2, 128}, {203, 2, 128}, {204, 2, 128}, {218, 2, 128}, {229, 2, 128},
-                                 {231, 2, 64}};
-    const bool half = precision == WT_F16 || precision == WT_BF16;
-    const int want = tile > 0 ? tile : (precision == WT_F64 ? 204 : (half && collision == WT_COLLIDE_FAST ? 231 : 229));
+                                 {118, 2, 128}, {203, 2, 128}, {204, 2, 128}, {218, 2, 128}, {229, 2, 128}};
+    const int want = tile > 0 ? tile : (precision == WT_F64 ? 204 : 229);
     for (const auto& r : ids)
         if (r[0] == want) {
             *v = r[1];
@@ -182,7 +179,7 @@ int launch_steps(wt_batch* b, int32_t steps, int32_t flags, cudaStream_t st) {
 extern "C" int64_t wt_batch_workspace_bytes(const wt_grid* grids, int32_t count, int32_t tile) {
     if (!grids || count <= 0) return wt_set_error(WT_ERR_ARG, "wt_batch_workspace_bytes: no tunnels");
     int v, block;
-    const int id = tile_shape(tile, grids[0].precision, grids[0].collision, &v, &block);
+    const int id = tile_shape(tile, grids[0].precision, &v, &block);
     if (!id) return wt_set_error(WT_ERR_ARG, "wt_batch: tile %d has no batched form", tile);
     const size_t ds = desc_bytes_for(grids[0].precision);
     if (!ds) return wt_set_error(WT_ERR_ARG, "wt_batch: unknown precision %d", grids[0].precision);
@@ -208,7 +205,7 @@ extern "C" int wt_batch_create(const wt_grid* grids, int32_t count, const double
         if (cur[t] != 0 && cur[t] != 1) return wt_set_error(WT_ERR_ARG, "wt_batch_create: cur of tunnel %d", t);
     }
     int v, block;
-    const int id = tile_shape(tile, prec, coll, &v, &block);
+    const int id = tile_shape(tile, prec, &v, &block);
     if (!id) return wt_set_error(WT_ERR_ARG, "wt_batch: tile %d has no batched form", tile);
     const BatchVariant* var = nullptr;
     switch (prec) {

@@ -41,8 +41,8 @@ static int launch_stream(const void* args, int32_t n, cudaStream_t st) {
 }
 
 // the row-grid arguments of one tunnel's step: its StepArgs plus the per-population byte offsets
-// of the pull and store and the blocks per row (runs of BLOCK pairs)
-template <class S, class T, int BLOCK>
+// of the pull and store
+template <class S, class T>
 static void fill_rows(RowArgs<S, T>& r, const StepArgs<S, T>& a) {
     r.a = a;
     for (int i = 0; i < Q; ++i) {
@@ -51,7 +51,6 @@ static void fill_rows(RowArgs<S, T>& r, const StepArgs<S, T>& a) {
         r.loff[i] = ((int64_t)i * a.n - (int64_t)cy(i) * a.nx - (int64_t)cz(i) * a.nxy) * (int64_t)sizeof(S);
         r.soff[i] = (int64_t)i * a.n * (int64_t)sizeof(S);
     }
-    r.druns = FastDiv((uint32_t)((a.nx / 2 + BLOCK - 1) / BLOCK));
 }
 
 template <int PREC, bool FAST, int BLOCK, int MINB, int ADDR, bool FUSE = false, bool EARLY = false>
@@ -61,7 +60,7 @@ static int launch_rows(const void* args, int32_t n, cudaStream_t st) {
     using T = typename P::T;
     (void)n;
     RowArgs<S, T> r;
-    fill_rows<S, T, BLOCK>(r, *static_cast<const StepArgs<S, T>*>(args));
+    fill_rows<S, T>(r, *static_cast<const StepArgs<S, T>*>(args));
     const StepArgs<S, T>& a = r.a;
     const dim3 grid((unsigned)((a.nx / 2 + BLOCK - 1) / BLOCK), (unsigned)a.ny, (unsigned)a.nz);
     k_step_rows<PREC, FAST, BLOCK, MINB, ADDR, FUSE, EARLY><<<grid, BLOCK, 0, st>>>(r);
@@ -128,18 +127,29 @@ const StepVariant* step_variants(bool fast, int* count) {
     return fast ? variants_of<PREC, true>(count) : variants_of<PREC, false>(count);
 }
 
-// defaults until the autotuner has measured the tunnel (the fastest shapes at 33.5M cells):
-// two cells per thread at 64 registers, as the one-dimensional tile 18 for fp32 and the
-// reference-order collision, as the row-grid tile 31 (64 threads, 16 blocks per SM, each pull
-// issued with its code bytes) for fp16 / bf16 storage with the moment-space collision; fp64
-// needs 128 registers to avoid spills, so it keeps two cells per thread at 128 registers
-// (tile 4)
+// defaults until the autotuner has measured the tunnel, chosen from timings of the benchmark body
+// at nx = 512, 320, 200 and 144: the row-grid tiles win where a lattice row splits into whole
+// blocks of pairs (each row's last block otherwise runs part-empty, and its partial warp takes
+// the general pair path), the one-dimensional two-cell tiles elsewhere. fp32 and the
+// reference-order collision: tile 34 (rows, 64 threads x 14 blocks, early pulls) when nx is a
+// multiple of 128, else tile 18. fp16 / bf16 with the moment-space collision: tile 31 (rows, 64
+// x 16, early pulls) when nx is a multiple of 128, tile 33 (rows, 32 x 32) when of 64, else tile
+// 29 (one-dimensional, early pulls). fp32 with the moment-space collision: tile 27 (rows, 128 x
+// 8, fused faces) when nx is a multiple of 256, else 18. Rows need nx >= 256 here: below that
+// the grid is too small to have been timed. fp64 needs 128 registers to avoid spills, so it
+// keeps two cells per thread at 128 registers (tile 4).
 template <int PREC>
 const StepVariant* pick_variant(const wt_grid* g) {
     int count;
     const bool fast = g->collision == WT_COLLIDE_FAST;
     const StepVariant* t = step_variants<PREC>(fast, &count);
-    const int dflt = PREC == WT_F64 ? 4 : ((PREC == WT_F16 || PREC == WT_BF16) && fast ? 31 : 18);
+    const bool half = PREC == WT_F16 || PREC == WT_BF16;
+    const bool big = g->nx >= 256;
+    int dflt = 18;
+    if (PREC == WT_F64) dflt = 4;
+    else if (fast && half) dflt = big && g->nx % 128 == 0 ? 31 : (big && g->nx % 64 == 0 ? 33 : 29);
+    else if (fast) dflt = big && g->nx % 256 == 0 ? 27 : 18;
+    else if (big && g->nx % 128 == 0) dflt = 34;
     const int want = g->tile > 0 ? g->tile : dflt;
     for (int k = 0; k < count; ++k) {
         if (t[k].id != want) continue;
@@ -332,50 +342,6 @@ __global__ void __launch_bounds__(FACE_BLOCK)
     face_cell<PREC>(bp.args[t], (b - bp.first[t]) * FACE_BLOCK + (int32_t)threadIdx.x);
 }
 
-// The row-grid body over many tunnels: the parameter block holds each tunnel's RowArgs (up to
-// MAXT of them); local block lb of a tunnel is x-run lb % runs of lattice row lb / runs.
-template <class S, class T>
-struct BatchRowParams {
-    static constexpr int MAXT = (32764 - 16) / (int)(sizeof(RowArgs<S, T>) + 4);
-    int32_t count;
-    int32_t first[MAXT + 1];
-    RowArgs<S, T> args[MAXT];
-};
-
-template <int PREC, bool FAST, int BLOCK, int MINB, bool EARLY>
-__global__ void __launch_bounds__(BLOCK, MINB)
-    k_batch_rows_params(const __grid_constant__ BatchRowParams<typename Prec<PREC>::S, typename Prec<PREC>::T> bp) {
-    const int32_t b = (int32_t)blockIdx.x;
-    const int32_t t = param_tunnel(bp, b);
-    const auto& r = bp.args[t];
-    const int32_t lb = b - bp.first[t];
-    const int32_t row = (int32_t)r.druns.div((uint32_t)lb);
-    const int32_t z = (int32_t)r.a.dny.div((uint32_t)row);
-    row_tile<PREC, FAST, BLOCK, 0, false, EARLY>(r, lb - row * (int32_t)r.druns.d, row - z * r.a.ny, z);
-}
-
-template <int PREC, bool FAST, int BLOCK, int MINB, bool EARLY>
-static int launch_batch_rows_params(const void* descs, int32_t count, cudaStream_t st) {
-    using S = typename Prec<PREC>::S;
-    using T = typename Prec<PREC>::T;
-    using BP = BatchRowParams<S, T>;
-    static_assert(sizeof(BP) <= 32764, "kernel parameters are limited to 32764 bytes");
-    const StepArgs<S, T>* d = static_cast<const StepArgs<S, T>*>(descs);
-    BP bp;
-    for (int32_t g0 = 0; g0 < count; g0 += BP::MAXT) {
-        const int32_t gc = std::min<int32_t>(count - g0, BP::MAXT);
-        bp.count = gc;
-        bp.first[0] = 0;
-        for (int32_t t = 0; t < gc; ++t) {
-            fill_rows<S, T, BLOCK>(bp.args[t], d[g0 + t]);
-            const StepArgs<S, T>& a = d[g0 + t];
-            bp.first[t + 1] = bp.first[t] + (int32_t)bp.args[t].druns.d * a.ny * a.nz;
-        }
-        k_batch_rows_params<PREC, FAST, BLOCK, MINB, EARLY><<<(unsigned)bp.first[gc], BLOCK, 0, st>>>(bp);
-    }
-    return WT_OK;
-}
-
 // FACES: the face kernel (FACE_BLOCK face cells per block) instead of the bulk one
 template <int PREC, bool FAST, int V, int BLOCK, int MINB, bool EARLY, bool FACES>
 static int launch_batch_params(const void* descs, int32_t count, cudaStream_t st) {
@@ -404,7 +370,7 @@ static int launch_batch_params(const void* descs, int32_t count, cudaStream_t st
 
 // the direct-load tile shapes of wt_step, same ids, as persistent kernels; ids 100 + k are
 // the grid forms of tile k, ids 200 + k the parameter-space forms (229: tile 18 with the pull
-// issued with the code bytes, as single-tunnel tile 29; 231: the row grid of tile 31)
+// issued with the code bytes, as single-tunnel tile 29)
 #define WT_BATCH_P(PREC, FAST, V, BLOCK, MINB, EARLY)                                                        \
     nullptr, nullptr, launch_batch_params<PREC, FAST, V, BLOCK, MINB, EARLY, false>,                          \
         launch_batch_params<PREC, FAST, V, BLOCK, MINB, EARLY, true>
@@ -423,9 +389,7 @@ static int launch_batch_params(const void* descs, int32_t count, cudaStream_t st
     {203, 2, 128, 6, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 6, false)},                                \
     {204, 2, 128, 4, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 4, false)},                                \
     {218, 2, 128, 8, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 8, false)},                                \
-    {229, 2, 128, 8, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 8, true)},                                 \
-    {231, 2, 64, 16, BATCH_PARAMS, nullptr, nullptr, launch_batch_rows_params<PREC, FAST, 64, 16, true>,        \
-     launch_batch_params<PREC, FAST, 2, 64, 16, true, true>}
+    {229, 2, 128, 8, BATCH_PARAMS, WT_BATCH_P(PREC, FAST, 2, 128, 8, true)}
 
 template <int PREC, bool FAST>
 const BatchVariant* batch_variant_of(int id) {

@@ -1129,7 +1129,6 @@ struct RowArgs {
     StepArgs<S, T> a;
     int64_t loff[Q];  // bytes from fin + idx0 to the aligned pull pair of population i
     int64_t soff[Q];  // bytes from fout + idx0 to population i of the output
-    FastDiv druns;    // blocks per lattice row (the parameter-space batch's block index to row)
 };
 
 template <int PREC, bool FAST>

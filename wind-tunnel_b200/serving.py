@@ -118,12 +118,10 @@ class SessionServer:
         self.collision = collision
         self.period = 1.0 / fps
         self.steps_per_frame = int(steps_per_frame)
-        # batched tile of the library executor: the parameter-space form (sessions step by their
-        # own counts) of the precision's fastest single-tunnel body: the row grid with early
-        # pulls for fp16 / bf16 with the moment-space collision (231), the two-cell tile with
-        # early pulls otherwise (229; at 128 registers, 204, for fp64)
-        half_fast = precision in ('fp16', 'bf16') and collision in (None, 'fast')
-        self.tile = int(tile) if tile else (204 if precision == 'fp64' else (231 if half_fast else 229))
+        # batched tile of the library executor: the parameter-space form of the two-cell tile
+        # with early pulls (229; 204, at 128 registers, for fp64), the fastest batched shape on
+        # config 4, which also steps sessions by their own counts
+        self.tile = int(tile) if tile else (204 if precision == 'fp64' else 229)
         # executor of the round's steps: every tunnel's own kernel on its own stream, all at
         # once ('streams'), or the library's batched kernels ('persistent': two launches per
         # step for all sessions)
