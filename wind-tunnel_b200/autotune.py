@@ -7,8 +7,8 @@ on a tunnel with CUDA events on the tunnel's stream and keeps the fastest; resul
 cached per (GPU, precision, grid) in memory and, when ``WT_TILE_CACHE`` names a file,
 in that JSON file.
 
-Timing advances the tunnel by ``len(tiles) * (warm + steps) * repeats`` LBM steps, so tune
-right after reset (as a warm-up) or on a scratch tunnel.
+Timing advances the tunnel by ``develop + len(tiles) * (warm + steps) * repeats`` LBM steps,
+so tune as a warm-up or on a scratch tunnel.
 """
 import json
 import os
@@ -69,13 +69,18 @@ def cached(solver):
     return hit['tile'] if hit else None
 
 
-def tune(solver, params, steps=8, warm=2, repeats=2, force=False):
-    """Pick the fastest tile for `solver` and set it; returns (tile, {tile: ms_per_step})."""
+def tune(solver, params, steps=8, warm=2, repeats=2, force=False, develop=0):
+    """Pick the fastest tile for `solver` and set it; returns (tile, {tile: ms_per_step}).
+    `develop` steps (with the current tile) come first, so the tiles are timed on a developed
+    flow: some tiles that are fastest right after a reset slow down by several percent once the
+    flow develops and others do not, so a fresh flow can rank them wrongly."""
     if not force:
         hit = cached(solver)
         if hit is not None:
             solver.set_tile(hit)
             return hit, _cache[_key(solver)]['ms']
+    if develop:
+        solver.step(develop, params)
     timings = {}
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
