@@ -7,8 +7,8 @@ on a tunnel with CUDA events on the tunnel's stream and keeps the fastest; resul
 cached per (GPU, precision, grid) in memory and, when ``WT_TILE_CACHE`` names a file,
 in that JSON file.
 
-Timing advances the tunnel by ``develop + len(tiles) * (warm + steps) * repeats`` LBM steps,
-so tune as a warm-up or on a scratch tunnel.
+Timing advances the tunnel by ``develop + len(tiles) * (warm + (warm + steps) * repeats)`` LBM
+steps, so tune as a warm-up or on a scratch tunnel.
 """
 import json
 import os
@@ -69,11 +69,15 @@ def cached(solver):
     return hit['tile'] if hit else None
 
 
-def tune(solver, params, steps=8, warm=2, repeats=2, force=False, develop=0):
+def tune(solver, params, steps=8, warm=2, repeats=3, force=False, develop=0):
     """Pick the fastest tile for `solver` and set it; returns (tile, {tile: ms_per_step}).
-    `develop` steps (with the current tile) come first, so the tiles are timed on a developed
-    flow: some tiles that are fastest right after a reset slow down by several percent once the
-    flow develops and others do not, so a fresh flow can rank them wrongly."""
+
+    Every tile is timed `repeats` times, the repeats interleaved across the tiles (all tiles
+    once, then all again), and ranked by its median: the SM clock falls as a run settles under
+    the power cap, so tiles timed one after another in a single pass would be ranked by their
+    place in the order as much as by their speed. `develop` steps (with the current tile) come
+    first, so the tiles are timed on a developed flow, in the state the steps that follow run in."""
+    import statistics
     if not force:
         hit = cached(solver)
         if hit is not None:
@@ -81,26 +85,26 @@ def tune(solver, params, steps=8, warm=2, repeats=2, force=False, develop=0):
             return hit, _cache[_key(solver)]['ms']
     if develop:
         solver.step(develop, params)
-    timings = {}
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    samples = {}
     for tile in admissible(solver):
-        tid = tile[0]
-        solver.set_tile(tid)
-        best = None
+        solver.set_tile(tile[0])
         try:
             solver.step(warm, params)
         except W.WtError:  # e.g. a streaming tile whose stages exceed shared memory
             continue
-        for _ in range(repeats):
+        samples[tile[0]] = []
+    for _ in range(repeats):
+        for tid, got in samples.items():
+            solver.set_tile(tid)
             solver.step(warm, params)
             ev0.record(solver.stream)
             solver.step(steps, params)
             ev1.record(solver.stream)
             ev1.synchronize()
-            ms = ev0.elapsed_time(ev1) / steps
-            best = ms if best is None else min(best, ms)
-        timings[tid] = best
+            got.append(ev0.elapsed_time(ev1) / steps)
+    timings = {tid: statistics.median(got) for tid, got in samples.items()}
     tid = min(timings, key=timings.get)
     solver.set_tile(tid)
     _cache[_key(solver)] = {'tile': tid, 'ms': timings}
