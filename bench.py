@@ -219,9 +219,10 @@ def run_ours(args, rank, world, local_rank):
         tile, tile_ms = args.tile, {}
         s.set_tile(tile)
     else:
-        # part of the warm-up, on a developed flow and in windows as long as the timed ones (the
-        # state the timed steps run in; 8-step bursts rank the heavier tiles too high)
-        tile, tile_ms = autotune.tune(s, p, force=True, develop=TUNE_DEVELOP, steps=STEP_CHUNK)
+        # part of the warm-up, on a developed flow, with the four fastest tiles of the screen run
+        # off in sustained windows (short windows under the power cap rank the heavier tiles too
+        # high)
+        tile, tile_ms = autotune.tune(s, p, force=True, develop=TUNE_DEVELOP, finalists=4)
     launches_per_frame = 2 * STEPS_PER_FRAME + 1 + 1 + 1 + 1 + 2  # steps, advect, pack, slice, cp, forces(2)
 
     def frame_device():
@@ -262,8 +263,9 @@ def run_ours(args, rank, world, local_rank):
                 'timing': f'median of {STEP_REPEATS} repeats of {STEP_CHUNK} steps (CUDA events on the tunnel stream)',
                 'step_ms_repeats': [round(x * 1e3, 4) for x in step_reps],
                 'tile_ms_per_step': {str(k): round(v, 4) for k, v in tile_ms.items()},
-                'tiles_timed': (f'by the autotuner after {TUNE_DEVELOP} steps of flow development, median of 3 '
-                                f'interleaved {STEP_CHUNK}-step windows per tile') if not args.tile
+                'tiles_timed': (f'by the autotuner after {TUNE_DEVELOP} steps of flow development: median of 3 '
+                                'interleaved 8-step windows per tile, then the 4 fastest in 3 interleaved '
+                                '100-step windows') if not args.tile
                                else 'tile given on the command line'}
     del s
     torch.cuda.empty_cache()
@@ -308,7 +310,7 @@ def run_ours(args, rank, world, local_rank):
             v = lbm.Solver(dims, dev, precision=vp, collision=vc)
             v.set_solid(solid)
             v.reset(p['uIn'])
-            vtile, vms = autotune.tune(v, p, force=True, develop=TUNE_DEVELOP, steps=STEP_CHUNK)
+            vtile, vms = autotune.tune(v, p, force=True, develop=TUNE_DEVELOP, finalists=4)
             v.step(5, p)
             tv, _ = step_time(v, p, ev0, ev1)
             variants[f'{vp}-{vc}'] = {'glups_step_only': round(n / tv / 1e9, 3),

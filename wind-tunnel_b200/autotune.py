@@ -8,7 +8,8 @@ cached per (GPU, precision, grid) in memory and, when ``WT_TILE_CACHE`` names a 
 in that JSON file.
 
 Timing advances the tunnel by ``develop + len(tiles) * (warm + (warm + steps) * repeats)`` LBM
-steps, so tune as a warm-up or on a scratch tunnel.
+steps (plus ``finalists * (warm + final_steps) * final_repeats``), so tune as a warm-up or on
+a scratch tunnel.
 """
 import json
 import os
@@ -69,15 +70,35 @@ def cached(solver):
     return hit['tile'] if hit else None
 
 
-def tune(solver, params, steps=8, warm=2, repeats=3, force=False, develop=0):
+def _interleaved(solver, params, tiles, steps, warm, repeats, ev0, ev1):
+    """Median ms per step of each tile over `repeats` windows of `steps` steps, the windows of
+    all tiles interleaved (all tiles once, then all again)."""
+    import statistics
+    got = {t: [] for t in tiles}
+    for _ in range(repeats):
+        for t in tiles:
+            solver.set_tile(t)
+            solver.step(warm, params)
+            ev0.record(solver.stream)
+            solver.step(steps, params)
+            ev1.record(solver.stream)
+            ev1.synchronize()
+            got[t].append(ev0.elapsed_time(ev1) / steps)
+    return {t: statistics.median(v) for t, v in got.items()}
+
+
+def tune(solver, params, steps=8, warm=2, repeats=3, force=False, develop=0, finalists=0, final_steps=100,
+         final_repeats=3):
     """Pick the fastest tile for `solver` and set it; returns (tile, {tile: ms_per_step}).
 
-    Every tile is timed `repeats` times, the repeats interleaved across the tiles (all tiles
-    once, then all again), and ranked by its median: the SM clock falls as a run settles under
-    the power cap, so tiles timed one after another in a single pass would be ranked by their
-    place in the order as much as by their speed. `develop` steps (with the current tile) come
-    first, so the tiles are timed on a developed flow, in the state the steps that follow run in."""
-    import statistics
+    Every admissible tile is timed `repeats` times in windows of `steps` steps, the windows
+    interleaved across the tiles, and ranked by its median. With `finalists`, the fastest few
+    then run off in longer interleaved windows (`final_steps`), and their entries in the returned
+    timings are those sustained figures. Under the GPU's power cap, short windows among lighter
+    tiles run at higher clocks than the same tile running on its own, and on this workload
+    that ranks a tile with more instructions per cell (one-dimensional tile 18) ahead of one
+    that is faster in sustained running (row tile 34). `develop` steps (with the current tile)
+    come first, so the tiles are timed on a developed flow."""
     if not force:
         hit = cached(solver)
         if hit is not None:
@@ -87,25 +108,21 @@ def tune(solver, params, steps=8, warm=2, repeats=3, force=False, develop=0):
         solver.step(develop, params)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    samples = {}
+    tiles = []
     for tile in admissible(solver):
         solver.set_tile(tile[0])
         try:
             solver.step(warm, params)
         except W.WtError:  # e.g. a streaming tile whose stages exceed shared memory
             continue
-        samples[tile[0]] = []
-    for _ in range(repeats):
-        for tid, got in samples.items():
-            solver.set_tile(tid)
-            solver.step(warm, params)
-            ev0.record(solver.stream)
-            solver.step(steps, params)
-            ev1.record(solver.stream)
-            ev1.synchronize()
-            got.append(ev0.elapsed_time(ev1) / steps)
-    timings = {tid: statistics.median(got) for tid, got in samples.items()}
-    tid = min(timings, key=timings.get)
+        tiles.append(tile[0])
+    timings = _interleaved(solver, params, tiles, steps, warm, repeats, ev0, ev1)
+    if finalists and len(tiles) > 1:
+        best = sorted(timings, key=timings.get)[:finalists]
+        timings.update(_interleaved(solver, params, best, final_steps, warm, final_repeats, ev0, ev1))
+        tid = min(best, key=timings.get)
+    else:
+        tid = min(timings, key=timings.get)
     solver.set_tile(tid)
     _cache[_key(solver)] = {'tile': tid, 'ms': timings}
     _save_file()
