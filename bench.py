@@ -171,6 +171,17 @@ def build_workload(scale):
     return dims, solid, verts, norms
 
 
+def step_kernels(tile):
+    """The kernels one step of step-tile `tile` launches (the tile table of csrc/wt_kernels.cuh)."""
+    if 8 <= tile <= 17:
+        return 'k_step_stream + k_step_faces'
+    if tile in (27, 28):
+        return 'k_step_rows with the face cells fused in'
+    if 19 <= tile <= 35 and tile != 29:
+        return 'k_step_rows + k_step_faces'
+    return 'k_step_bulk + k_step_faces'
+
+
 STEP_REPEATS, STEP_CHUNK = 5, 50
 TUNE_DEVELOP = 1000  # steps of flow development before the autotuner times the tiles
 
@@ -256,7 +267,7 @@ def run_ours(args, rank, world, local_rank):
     roofline = {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': hbm, 'unit': 'GB/s',
                 'frac': round(achieved / hbm, 4), 'traffic': traffic,
                 'peak_source': f'{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)' if peak_kind == 'measured'
-                else 'fallback 6.65 TB/s', 'kernel': f'wt_step ({prec}) = k_step_bulk + k_step_faces, one LBM step',
+                else 'fallback 6.65 TB/s', 'kernel': f'wt_step ({prec}) = {step_kernels(tile)}, one LBM step',
                 'algorithmic_bytes_per_cell': ALGO_BYTES[prec], 'step_ms': round(t_step * 1e3, 4),
                 'copy_gbs_this_run': round(copy_here, 1), 'frac_of_copy_this_run': round(achieved / copy_here, 4),
                 'glups_step_only': round(n / t_step / 1e9, 3), 'tile': tile,
