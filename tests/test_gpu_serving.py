@@ -222,3 +222,38 @@ def test_recycled_tunnel_equals_a_new_one(precision):
     assert got['recycled'][0] == got['new'][0]
     assert np.array_equal(got['recycled'][1], got['new'][1])
     assert np.array_equal(got['recycled'][2], got['new'][2])
+
+
+@pytest.mark.parametrize('precision', ['fp32', 'fp16'])
+def test_solver_on_arena_storage_equals_a_plain_one(precision):
+    """A Solver whose per-cell state is a range of the serving arena (filled with garbage first,
+    next to another dirty range) gives the frames and populations of a Solver that allocated
+    its own."""
+    import arena
+    import lbm
+    s0 = _sessions()[2]
+    _, total = lbm.state_layout(s0.dims, precision)
+    a = arena.Arena(3 * total + 4096, 'cuda:0')
+    other, off = a.alloc(total), a.alloc(total)
+    a.view(other, total).fill_(0x5a)
+    a.view(off, total).fill_(0xa5)
+
+    def run(sv):
+        sv.set_solid(s0.solid)
+        sv.reset(s0.p['uIn'])
+        sv.set_particles(s0.particles, s0.p)
+        out = []
+        for _ in range(3):
+            sv.step(7, s0.p)
+            sv.advance_particles(7, s0.p)
+            sv.launch_frame_packed(s0.p, False)
+            header = dict(type='frame', dims=list(s0.dims), numP=sv.num_p, numVerts=0, forces=None, steps=7,
+                          mlups=0.0, running=True)
+            out.append(sv.collect_frame_packed(header))
+        return out, sv.populations(), sv.macro()
+
+    on_arena = run(lbm.Solver(s0.dims, 'cuda:0', precision=precision, seed=s0.id, storage=a.view(off, total)))
+    plain = run(lbm.Solver(s0.dims, 'cuda:0', precision=precision, seed=s0.id))
+    assert on_arena[0] == plain[0]
+    assert np.array_equal(on_arena[1], plain[1]) and np.array_equal(on_arena[2], plain[2])
+    assert bool((a.view(other, total) == 0x5a).all())  # the neighbouring range is untouched

@@ -548,3 +548,41 @@ def test_at_most_new_per_round_tunnels_are_allocated_each_round():
     c.t = 1.2
     srv.round()  # the next round allocates 3
     assert list(srv.active) == [1, 2, 3] and RecyclingSolver.made == 3
+
+
+def test_arena_ranges_follow_the_tunnels_and_an_arrival_waits_for_a_range():
+    import arena
+    c = Clock()
+    unit = 256
+
+    def factory(s):  # the default factory's arena use, with fake tunnels
+        if s.reuse is not None:
+            sv, s.reuse = s.reuse, None
+            sv.recycle(s.id)
+            sv.s = s
+            return sv
+        off = srv._arena.alloc(s.n * unit)
+        assert off is not None
+        sv = RecyclingSolver(s)
+        sv.arena_off = off
+        return sv
+
+    srv = _server(c, budget=100, solver_factory=factory, arena=True)
+    srv._arena = arena.Arena(10 * unit)
+    srv._state_bytes = lambda s: s.n * unit
+    srv._allocate = lambda s: None  # marks the default path; admission here builds in the round
+    a, b, d = _session(0, 4, life=1.0), _session(1, 4), _session(2, 3)
+    for s in (a, b, d):
+        srv.submit(s)
+    srv.round()
+    # the budget (100) has room for the third, the arena (2 units free) has not
+    assert list(srv.active) == [0, 1] and [s.id for s in srv.queue] == [2] and srv.arena_waits == 1
+    c.t = 1.0  # session 0 retires and its tunnel is kept; then session 2, of another grid, needs
+    srv.round()  # a range: the kept tunnel is dropped and its range reused
+    assert list(srv.active) == [1, 2] and srv.pool_evictions == 1 and srv.pooled == 0
+    assert srv._arena.used == {0: 3 * unit, 4 * unit: 4 * unit}
+    c.t = 2.0
+    srv.disconnect(1)
+    srv.disconnect(2)
+    srv.round()
+    srv.close()

@@ -60,6 +60,23 @@ def estimate_bytes(dims, precision='fp32', particles=0, num_verts=0):
             + num_verts * 26 + 8 * int(W.lib().wt_reduce_scratch_len(0)) + 4096)
 
 
+def state_layout(dims, precision='fp32'):
+    """Byte offsets of a Solver's per-cell state in one block of device memory (the two
+    population buffers, the two mac buffers, solid and code, each 256-byte aligned), and the
+    block's size: {'f0': (offset, bytes), ...}, total."""
+    prec = W.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    nx, ny, nz = (int(d) for d in dims)
+    n = nx * ny * nz
+    mac = 32 if prec == W.F64 else 16
+    parts = [('f0', Q * n * _POP_BYTES[prec]), ('f1', Q * n * _POP_BYTES[prec]), ('mac0', n * mac), ('mac1', n * mac),
+             ('solid', n), ('code', n)]
+    out, off = {}, 0
+    for name, nbytes in parts:
+        out[name] = (off, nbytes)
+        off += (nbytes + 255) // 256 * 256
+    return out, off
+
+
 def _device(device):
     if not torch.cuda.is_available():
         raise RuntimeError('wind-tunnel_b200 needs a CUDA device; there is no CPU path')
@@ -85,7 +102,7 @@ class Solver:
     """
 
     def __init__(self, dims, device=None, precision='fp32', stream=None, seed=None, collision=None,
-                 shift='free-stream'):
+                 shift='free-stream', storage=None):
         self.dev = _device(device)
         self.nx, self.ny, self.nz = (int(d) for d in dims)
         self.n = n = self.nx * self.ny * self.nz
@@ -107,10 +124,25 @@ class Solver:
         mac_dt = torch.float64 if self.precision == W.F64 else torch.float32
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
             # zero-filled like the reference's wp.zeros buffers (server/lbm.py:404-407)
-            self.f = [torch.zeros(Q * n, dtype=_TORCH_POP[self.precision], device=self.dev) for _ in range(2)]
-            self.mac = [torch.zeros((n, 4), dtype=mac_dt, device=self.dev) for _ in range(2)]
-            self.solid = torch.zeros(n, dtype=torch.uint8, device=self.dev)
-            self.code = torch.zeros(n, dtype=torch.uint8, device=self.dev)
+            if storage is None:
+                self.f = [torch.zeros(Q * n, dtype=_TORCH_POP[self.precision], device=self.dev) for _ in range(2)]
+                self.mac = [torch.zeros((n, 4), dtype=mac_dt, device=self.dev) for _ in range(2)]
+                self.solid = torch.zeros(n, dtype=torch.uint8, device=self.dev)
+                self.code = torch.zeros(n, dtype=torch.uint8, device=self.dev)
+            else:
+                # the per-cell state in a caller's block of device memory (uint8, 256-byte aligned,
+                # state_layout's size at least), e.g. a range of a serving arena
+                layout, total = state_layout(dims, self.precision)
+                if storage.dtype != torch.uint8 or storage.dim() != 1 or storage.numel() < total:
+                    raise ValueError(f'storage must be a 1-D uint8 tensor of at least {total} bytes')
+                if storage.device != self.dev or storage.data_ptr() % 256:
+                    raise ValueError('storage must be 256-byte aligned memory on the Solver\'s device')
+                part = {k: storage[o:o + nb] for k, (o, nb) in layout.items()}
+                self.f = [part[k].view(_TORCH_POP[self.precision]) for k in ('f0', 'f1')]
+                self.mac = [part[k].view(mac_dt).view(n, 4) for k in ('mac0', 'mac1')]
+                self.solid, self.code = part['solid'], part['code']
+                for t in (*self.f, *self.mac, self.solid, self.code):
+                    t.zero_()
             self.forces_dev = torch.zeros(6, dtype=torch.float64, device=self.dev)
             self.mass_dev = torch.zeros(1, dtype=torch.float64, device=self.dev)
             self.status_dev = torch.zeros(1, dtype=torch.int32, device=self.dev)

@@ -111,7 +111,7 @@ class SessionServer:
                  tile=0, collision=None, clock=time.perf_counter, solver_factory=None, batch_factory=None,
                  footprint=None, keep_frames=False, batch_mode='streams', pacing='fps', paused_hz=PAUSED_HZ,
                  rate_in_header=True, priorities=True, work_bound_glups=None, admit_thread=False, recycle=True,
-                 new_per_round=None):
+                 new_per_round=None, arena=None):
         self.device = device
         self.budget = float(budget_bytes)
         self.precision = precision
@@ -133,6 +133,13 @@ class SessionServer:
         # the GPU is idle between rounds (an allocator that frees its cache synchronises the
         # device, and allocation holds driver locks), and initialised on the worker thread
         self._allocate = self._alloc_solver if solver_factory is None else None
+        # arena: the default factory's tunnels take their per-cell state from one block of device
+        # memory the size of the budget (arena.py), allocated at the first admission, so that
+        # admitting and dropping tunnels makes no CUDA allocation; on by default with it
+        self.use_arena = (solver_factory is None) if arena is None else bool(arena)
+        self._arena = None
+        self._released = collections.deque()  # tunnels a failed build left, to give back
+        self.arena_waits = 0
         self.batch_factory = batch_factory or self._make_batch
         self.footprint = footprint or (lambda s: lbm.estimate_bytes(s.dims, precision, s.particles))
         self.keep_frames = keep_frames
@@ -233,33 +240,67 @@ class SessionServer:
             return 0
         return -3 if s.n <= 1_000_000 else (-2 if s.n <= 4_000_000 else (-1 if s.n <= 16_000_000 else 0))
 
+    def _arena_get(self):
+        if self._arena is None:
+            import arena
+            self._arena = arena.Arena(self.budget, self.device)
+        return self._arena
+
+    def _state_bytes(self, s):
+        return lbm.state_layout(s.dims, self.precision)[1]
+
+    def _drop_solver(self, sv):
+        """A tunnel leaves for good: its arena range goes back."""
+        off = getattr(sv, 'arena_off', None)
+        if off is not None:
+            self._arena.release(off)
+            sv.arena_off = None
+
     def _alloc_solver(self, s):
-        """A new tunnel's device and pinned frame buffers (lbm.Solver), on its own stream."""
+        """A new tunnel's device and pinned frame buffers (lbm.Solver), on its own stream, its
+        per-cell state in a range of the arena when the server uses one."""
         import torch
-        stream = torch.cuda.Stream(torch.device(self.device), priority=self._priority(s))
-        sv = lbm.Solver(s.dims, self.device, precision=self.precision, collision=self.collision, seed=s.id,
-                        stream=stream)
-        sv.prepare_frame(s.p, s.verts is not None)
+        off, storage = None, None
+        if self.use_arena:
+            a = self._arena_get()
+            total = self._state_bytes(s)
+            off = a.alloc(total)
+            if off is None:
+                raise MemoryError(f'no free range of {total} bytes in the tunnel arena')
+            storage = a.view(off, total)
+        try:
+            stream = torch.cuda.Stream(torch.device(self.device), priority=self._priority(s))
+            sv = lbm.Solver(s.dims, self.device, precision=self.precision, collision=self.collision, seed=s.id,
+                            stream=stream, storage=storage)
+            sv.prepare_frame(s.p, s.verts is not None)
+        except Exception:
+            if off is not None:
+                self._arena.release(off)
+            raise
+        sv.arena_off = off
         sv.fresh = True
         return sv
 
     def _make_solver(self, s):
         if s.reuse is not None:  # a kept tunnel of this grid, or one allocated at admission
             sv, s.reuse = s.reuse, None
+        else:
+            sv = self._alloc_solver(s)
+        try:
             if not getattr(sv, 'fresh', False):
                 sv.recycle(seed=s.id)
             sv.fresh = False
-        else:
-            sv = self._alloc_solver(s)
-            sv.fresh = False
-        sv.set_solid(s.solid)
-        sv.reset(s.p['uIn'])
-        if s.particles:
-            sv.set_particles(s.particles, s.p)
-        if s.verts is not None:
-            sv.set_surface(s.verts, s.norms)
-        sv.prepare_frame(s.p, s.verts is not None)
-        sv.synchronize()
+            sv.set_solid(s.solid)
+            sv.reset(s.p['uIn'])
+            if s.particles:
+                sv.set_particles(s.particles, s.p)
+            if s.verts is not None:
+                sv.set_surface(s.verts, s.norms)
+            sv.prepare_frame(s.p, s.verts is not None)
+            sv.synchronize()
+        except Exception:
+            self._released.append(sv)  # the serving thread gives its arena range back
+            raise
         return sv
 
     def _make_batch(self, solvers, params):
@@ -417,6 +458,8 @@ class SessionServer:
 
     def _admit(self, now):
         allocated = 0
+        while self._released:
+            self._drop_solver(self._released.popleft())
         while self._built:  # tunnels the worker finished join this round
             s, err = self._built.popleft()
             del self.building[s.id]
@@ -444,6 +487,13 @@ class SessionServer:
             kept = self._pool.get(key)
             if not kept and self.new_per_round is not None and allocated >= self.new_per_round:
                 break  # the next round allocates it
+            if not kept and self.use_arena and self._allocate is not None:
+                total = self._state_bytes(s)
+                if self._arena_get().largest() < total:  # kept tunnels give their ranges back
+                    self._evict_for_range(total)
+                    if self._arena.largest() < total:
+                        self.arena_waits += 1
+                        break
             reuse_bytes = kept[-1][1] if kept else 0.0
             over = self.used + self.pooled - reuse_bytes + max(need, reuse_bytes) - self.budget
             if over > 0:  # drop kept tunnels, never the one this session would take
@@ -508,6 +558,7 @@ class SessionServer:
             s.solver.synchronize()
         except Exception:
             pass
+        self._drop_solver(s.solver)
         s.solver = None
         self.failed += 1
         self.errors.append((s.id, f'solver error: {err!r}'))
@@ -527,6 +578,8 @@ class SessionServer:
             if self.recycle and hasattr(s.solver, 'recycle'):
                 self._pool.setdefault(self._pool_key(s), []).append((s.solver, s.bytes))
                 self.pooled += s.bytes
+            else:
+                self._drop_solver(s.solver)
             s.solver = None
             self.retired += 1
 
@@ -546,7 +599,21 @@ class SessionServer:
             need -= self._pool[k][j][1]
             drop.append((k, j))
         for k, j in sorted(drop, key=lambda kj: -kj[1]):
-            _, b = self._pool[k].pop(j)
+            sv, b = self._pool[k].pop(j)
+            self._drop_solver(sv)
+            self.pooled -= b
+            self.pool_evictions += 1
+            if not self._pool[k]:
+                del self._pool[k]
+
+    def _evict_for_range(self, total):
+        """Drop kept tunnels, the largest first, until the arena has a free range of `total`
+        bytes."""
+        while self._pool and self._arena.largest() < total:
+            k, j = max(((k, j) for k, v in self._pool.items() for j in range(len(v))),
+                       key=lambda kj: self._pool[kj[0]][kj[1]][1])
+            sv, b = self._pool[k].pop(j)
+            self._drop_solver(sv)
             self.pooled -= b
             self.pool_evictions += 1
             if not self._pool[k]:
@@ -685,6 +752,9 @@ class SessionServer:
                 'max_queued': self.max_queued, 'used_gb_end': round(self.used / 1e9, 2),
                 'kept_gb_end': round(self.pooled / 1e9, 2), 'tunnels_reused': self.pool_hits,
                 'kept_tunnels_dropped': self.pool_evictions,
+                'arena_gb': None if self._arena is None else round(self._arena.size / 1e9, 2),
+                'arena_largest_free_gb_end': None if self._arena is None else round(self._arena.largest() / 1e9, 2),
+                'arena_waits': self.arena_waits,
                 'peak_used_gb': round(self.peak_used / 1e9, 2),
                 'glups': round(self.cell_updates / span / 1e9, 3),
                 'step_glups_device': round(self.step_cells / max(1e-9, self.step_gpu_s) / 1e9, 3),
@@ -746,6 +816,10 @@ class SessionServer:
         self.active.clear()
         self._pool.clear()
         self.pooled = 0.0
+        if self._arena is not None:  # every tunnel is gone: the arena's memory goes back
+            import torch
+            self._arena = None
+            torch.cuda.empty_cache()
 
 
 # ---- config 5: Poisson arrivals of tunnels of four sizes ----
