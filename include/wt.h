@@ -68,7 +68,8 @@ typedef struct wt_grid {
     void* mac[2];          /* two macroscopic buffers, 4*n reals each (double-buffered) */
     const uint8_t* solid;  /* n bytes, reference mask semantics */
     uint8_t* code;         /* n bytes, filled by wt_build_codes from solid */
-    int32_t tile;          /* step kernel tile variant (wt_step_tiles); 0 = library default */
+    int32_t tile;          /* step kernel tile variant (wt_step_tiles); 0 = library default, by
+                              precision, collision form and nx */
     int32_t collision;     /* WT_COLLIDE_EXACT (reference operation order) or WT_COLLIDE_FAST */
     int32_t* status;       /* optional device int: set to WT_ERR_TIMEOUT if a bounded wait gives up */
     float shift_u;         /* fp16/bf16 storage shift velocity U (see WT_F16); ignored otherwise.
@@ -153,8 +154,8 @@ int wt_forces_noalloc(const wt_grid* g, int32_t cur, const int32_t* cells, const
 int wt_mass(const wt_grid* g, int32_t cur, double* partials, double* out1, void* stream);
 
 /* ---- many tunnels at once ----
- * A batch advances `count` tunnels of uneven sizes together: per step one bulk kernel over a
- * tile work-list spanning all tunnels, then one kernel over all tunnels' face cells. No
+ * A batch advances `count` tunnels of uneven sizes together: per step one bulk kernel over all
+ * tunnels' cells, then one kernel over all tunnels' face cells. No
  * counterpart in the reference, which runs one tunnel (server/app.py:116); each tunnel's
  * results are bit-identical to stepping it alone with wt_step. All tunnels share precision and
  * collision form. tile selects the shape: a direct-load tile id k of wt_step_tiles (1-5, 7, 18)
