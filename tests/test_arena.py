@@ -1,6 +1,6 @@
-"""The serving arena's ranges (host logic; no GPU): first fit from the bottom and last fit from
-the top at 256-byte alignment, merging of freed neighbours, and a random sequence of
-allocations and releases checked against a byte-occupancy model."""
+"""The serving arena's ranges (host logic; no GPU): first fit at 256-byte alignment, merging of
+freed neighbours, and a random sequence of allocations and releases checked against a
+byte-occupancy model."""
 import random
 
 import arena
@@ -37,13 +37,10 @@ def test_random_sequence_matches_an_occupancy_model():
             a.release(off)
         else:
             n = rng.randrange(1, 6000)
-            high = rng.random() < 0.3
-            off = a.alloc(n, high=high)
+            off = a.alloc(n)
             need = (n + 255) // 256 * 256
-            if high:  # last fit: the highest free window, the end of the last run that holds `need` bytes
-                first = next((o for o in range(a.size - need, -1, -256) if not any(occ[o:o + need])), None)
-            else:  # first fit: no earlier free run of `need` bytes at a 256-byte boundary exists
-                first = next((o for o in range(0, a.size - need + 1, 256) if not any(occ[o:o + need])), None)
+            # first fit: no earlier free run of `need` bytes at a 256-byte boundary exists
+            first = next((o for o in range(0, a.size - need + 1, 256) if not any(occ[o:o + need])), None)
             assert off == first
             if off is not None:
                 assert off % 256 == 0 and not any(occ[off:off + need])
@@ -61,12 +58,3 @@ def test_random_sequence_matches_an_occupancy_model():
             runs.append((o, e - o))
             o = e
         assert a.free == runs
-
-
-def test_large_blocks_from_the_top():
-    a = arena.Arena(10 * 256)
-    small = a.alloc(256)
-    big = a.alloc(3 * 256, high=True)
-    assert (small, big) == (0, 7 * 256) and a.free == [(256, 6 * 256)]
-    a.release(big)
-    assert a.free == [(256, 9 * 256)]

@@ -4,9 +4,9 @@ A SessionServer admits tunnels of a few sizes against an HBM budget, and they co
 every second. Left to torch's caching allocator, tunnels of different sizes fragment its
 cache, and an allocation that finds no fitting block makes the allocator free its cache
 (synchronising the device) and call cudaMalloc. Under a nearly full budget that took 400-600
-ms of a serving round. The arena is allocated once, and tunnels take ranges of it at 256-byte
-alignment, small ones by first fit from the bottom and large ones by last fit from the top;
-freed ranges merge with free neighbours. No CUDA allocation or free happens per tunnel.
+ms of a serving round. The arena is allocated once, and tunnels take ranges of it by first
+fit at 256-byte alignment; freed ranges merge with free neighbours. No CUDA allocation or free
+happens per tunnel.
 
 ``Arena(nbytes)`` keeps only the ranges (host logic, testable without a GPU);
 ``Arena(nbytes, device)`` also holds the device buffer, and ``view(offset, nbytes)`` returns
@@ -38,25 +38,18 @@ class Arena:
     def free_bytes(self):
         return sum(n for _, n in self.free)
 
-    def alloc(self, nbytes, high=False):
-        """Offset of a range of `nbytes` (rounded up to 256), or None: the start of the first free
-        range that fits, or with `high` the end of the last one, so that large blocks taken from
-        the top and small ones from the bottom do not interleave."""
+    def alloc(self, nbytes):
+        """Offset of a range of `nbytes` (rounded up to 256), the first free one that fits, or
+        None."""
         need = _round(nbytes)
-        order = range(len(self.free) - 1, -1, -1) if high else range(len(self.free))
-        for k in order:
-            off, n = self.free[k]
-            if n < need:
-                continue
-            if n == need:
-                del self.free[k]
-            elif high:
-                self.free[k] = (off, n - need)
-                off += n - need
-            else:
-                self.free[k] = (off + need, n - need)
-            self.used[off] = need
-            return off
+        for k, (off, n) in enumerate(self.free):
+            if n >= need:
+                if n == need:
+                    del self.free[k]
+                else:
+                    self.free[k] = (off + need, n - need)
+                self.used[off] = need
+                return off
         return None
 
     def release(self, off):

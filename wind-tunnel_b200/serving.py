@@ -249,11 +249,6 @@ class SessionServer:
     def _state_bytes(self, s):
         return lbm.state_layout(s.dims, self.precision)[1]
 
-    def _high(self, total):
-        """Tunnels of at least 1/32 of the arena (the 33.5M-cell class under a 160 GB budget)
-        are placed from the top, the rest from the bottom."""
-        return total * 32 >= self._arena.size
-
     def _drop_solver(self, sv):
         """A tunnel leaves for good: its arena range goes back."""
         off = getattr(sv, 'arena_off', None)
@@ -269,7 +264,7 @@ class SessionServer:
         if self.use_arena:
             a = self._arena_get()
             total = self._state_bytes(s)
-            off = a.alloc(total, high=self._high(total))
+            off = a.alloc(total)
             if off is None:
                 raise MemoryError(f'no free range of {total} bytes in the tunnel arena')
             storage = a.view(off, total)
